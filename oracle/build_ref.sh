@@ -1,0 +1,53 @@
+#!/usr/bin/env bash
+# Builds the reference's own CPU hot-path code (Vlasiator, GPL-2.0-or-later)
+# into oracle/_ref/ as a parity oracle and CPU baseline.  Nothing from the
+# reference is copied into this repository: the reference sources are
+# symlinked from where they lie into a build tree under oracle/_ref/src, the
+# few headers that pull in MPI / dccrg / phiprof are replaced by the small
+# stand-ins in oracle/ref_shim, and only the shared objects are written.
+#
+#   oracle/_ref/libvlasov_ref_sp.so  : FP32 VDF (Realf=float, Real=double), VECL=16, PPM
+#   oracle/_ref/libvlasov_ref_dp.so  : all-FP64 (Realf=double), VECL=8, PPM
+#
+# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${1:-/root/reference}"
+OUT="$HERE/_ref"
+SRC="$OUT/src"
+if [ ! -f "$REF/vlasovsolver/cpu_acc_map.cpp" ]; then
+  echo "build_ref: reference tree not found at $REF" >&2
+  exit 3
+fi
+rm -rf "$SRC"
+mkdir -p "$SRC/vlasovsolver" "$SRC/spatial_cells" "$SRC/arch" "$SRC/sysinc"
+for f in cpu_acc_map.cpp cpu_acc_map.hpp cpu_acc_sort_blocks.cpp cpu_acc_sort_blocks.hpp \
+         cpu_acc_load_blocks.cpp cpu_acc_load_blocks.hpp cpu_1d_plm.hpp cpu_1d_ppm.hpp \
+         cpu_1d_pqm.hpp cpu_1d_ppm_nonuniform.hpp cpu_face_estimates.hpp cpu_slope_limiters.hpp \
+         vec.h vectorclass_fallback.h arch_moments.h; do
+  ln -s "$REF/vlasovsolver/$f" "$SRC/vlasovsolver/$f"
+done
+for f in velocity_mesh_cpu.h velocity_block_container.h; do
+  ln -s "$REF/spatial_cells/$f" "$SRC/spatial_cells/$f"
+done
+for f in common.h definitions.h open_bucket_hashtable.h velocity_mesh_parameters.h velocity_mesh_parameters.cpp memoryallocation.h; do
+  ln -s "$REF/$f" "$SRC/$f"
+done
+for f in arch_device_api.h arch_device_host.h; do
+  ln -s "$REF/arch/$f" "$SRC/arch/$f"
+done
+cp "$HERE/ref_shim/object_wrapper.h" "$SRC/object_wrapper.h"
+cp "$HERE/ref_shim/spatial_cells/spatial_cell_wrapper.hpp" "$SRC/spatial_cells/spatial_cell_wrapper.hpp"
+cp "$HERE/ref_shim/sysinc/"*.hpp "$SRC/sysinc/"
+cp "$HERE/ref_harness.cpp" "$SRC/ref_harness.cpp"
+
+CXX="${REF_CXX:-/usr/bin/g++}"
+COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
+        -DDP -DACC_SEMILAG_PPM -DTRANS_SEMILAG_PPM -DVEC_FALLBACK_GENERIC
+        -I"$SRC" -I"$SRC/sysinc" -w)
+SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
+      "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
+      "$SRC/velocity_mesh_parameters.cpp")
+"$CXX" "${COMMON[@]}" -DSPF -DVECL=16 "${SRCS[@]}" -o "$OUT/libvlasov_ref_sp.so"
+"$CXX" "${COMMON[@]}" -DDPF -DVECL=8 "${SRCS[@]}" -o "$OUT/libvlasov_ref_dp.so"
+echo "build_ref: built $OUT/libvlasov_ref_sp.so $OUT/libvlasov_ref_dp.so"

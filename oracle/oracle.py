@@ -1,0 +1,178 @@
+"""ctypes bindings for the parity oracle (test infrastructure only).
+
+Two back ends:
+
+* ``Restatement`` -- ``oracle/liborc_{sp,dp}.so`` built from vlasov_oracle.c,
+  the plain-C restatement of the reference's algorithm.
+* ``ReferenceBuild`` -- ``oracle/_ref/libvlasov_ref_{sp,dp}.so`` built by
+  oracle/build_ref.sh from the reference's own sources; present only where the
+  reference tree was available at build time.
+
+Only tests, the smoke check and bench.py's CPU-baseline leg import this.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from vlasiator_b200.mesh import WID3, CMesh, VelocityMesh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def build(with_reference: bool = False) -> None:
+    """Compiles the restatement (and, if asked and available, the reference build)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if with_reference and os.path.isdir("/root/reference/vlasovsolver"):
+        subprocess.run([os.path.join(HERE, "build_ref.sh")], check=True, stdout=subprocess.DEVNULL)
+
+
+class Restatement:
+    def __init__(self, precision: str = "sp"):
+        path = os.path.join(HERE, f"liborc_{precision}.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = ctypes.CDLL(path)
+        self.realf = np.float32 if precision == "sp" else np.float64
+        ct = ctypes.c_float if precision == "sp" else ctypes.c_double
+        self._ct = ct
+        L = self.lib
+        L.orc_map_1d.restype = ctypes.c_int
+        L.orc_map_1d.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_uint32, ctypes.c_double,
+                                 ctypes.c_uint32, ctypes.c_uint32, _u32p, _u32p, ctypes.POINTER(ct), _u32p]
+        L.orc_acceleration_transform.restype = None
+        L.orc_acceleration_transform.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                 ctypes.c_double, _dp, _dp]
+        L.orc_cell_intersections.restype = None
+        L.orc_cell_intersections.argtypes = [_dp, _dp, ctypes.POINTER(CMesh), ctypes.c_uint32, _dp]
+
+    def map_1d(self, mesh: VelocityMesh, gids, data, isect4, dim: int, min_value: float, wall_margin: int = 1,
+               cap: int | None = None):
+        gids = np.ascontiguousarray(gids, dtype=np.uint32)
+        data = np.ascontiguousarray(data, dtype=self.realf).reshape(-1, WID3)
+        cap = cap or max(4 * len(gids) + 4096, 8192)
+        go = np.zeros(cap, np.uint32)
+        do = np.zeros((cap, WID3), self.realf)
+        n = ctypes.c_uint32(0)
+        fl = ctypes.c_uint32(0)
+        cm = CMesh.of(mesh)
+        rc = self.lib.orc_map_1d(ctypes.byref(cm), len(gids), _ptr(gids, ctypes.c_uint32), _ptr(data, self._ct),
+                                 float(isect4[0]), float(isect4[1]), float(isect4[2]), float(isect4[3]), dim,
+                                 float(min_value), wall_margin, cap, ctypes.byref(n), _ptr(go, ctypes.c_uint32),
+                                 _ptr(do, self._ct), ctypes.byref(fl))
+        if rc != 0:
+            raise RuntimeError(f"orc_map_1d failed with status {rc}")
+        return go[: n.value].copy(), do[: n.value].copy(), fl.value
+
+    def acceleration_transform(self, B, curl, rhoq, V, egradpe, q, m, dt, hall_min_rhoq, ohm_gradpe, mu0):
+        L = np.zeros(9)
+        t = np.zeros(3)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        curl = np.ascontiguousarray(curl, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        eg = np.ascontiguousarray(egradpe, dtype=np.float64)
+        self.lib.orc_acceleration_transform(_ptr(B, ctypes.c_double), _ptr(curl, ctypes.c_double), float(rhoq),
+                                            _ptr(V, ctypes.c_double), _ptr(eg, ctypes.c_double), float(q), float(m),
+                                            float(dt), float(hall_min_rhoq), int(ohm_gradpe), float(mu0),
+                                            _ptr(L, ctypes.c_double), _ptr(t, ctypes.c_double))
+        return L.reshape(3, 3), t
+
+    def cell_intersections(self, L, t, mesh: VelocityMesh, map_order: int):
+        L = np.ascontiguousarray(L, dtype=np.float64).reshape(9)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        out = np.zeros(12)
+        cm = CMesh.of(mesh)
+        self.lib.orc_cell_intersections(_ptr(L, ctypes.c_double), _ptr(t, ctypes.c_double), ctypes.byref(cm),
+                                        map_order, _ptr(out, ctypes.c_double))
+        return out
+
+
+def reference_available(precision: str = "sp") -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libvlasov_ref_{precision}.so"))
+
+
+class ReferenceBuild:
+    """The reference's own map_1d and moment templates, driven through oracle/ref_harness.cpp."""
+
+    _mesh_set = {}
+
+    def __init__(self, precision: str = "sp"):
+        path = os.path.join(HERE, "_ref", f"libvlasov_ref_{precision}.so")
+        self.lib = ctypes.CDLL(path)
+        self.realf = np.float32 if precision == "sp" else np.float64
+        ct = ctypes.c_float if precision == "sp" else ctypes.c_double
+        self._ct = ct
+        L = self.lib
+        L.ref_init.argtypes = [_dp, _dp, _u32p, ctypes.c_uint32]
+        L.ref_cells_create.restype = _vp
+        L.ref_cells_create.argtypes = [ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64), _u32p, ctypes.POINTER(ct), _dp]
+        L.ref_cells_destroy.argtypes = [_vp]
+        L.ref_cells_block_count.restype = ctypes.c_uint64
+        L.ref_cells_block_count.argtypes = [_vp, ctypes.c_uint32]
+        L.ref_cells_extract.restype = ctypes.c_uint64
+        L.ref_cells_extract.argtypes = [_vp, ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_uint64]
+        L.ref_cells_map_1d.argtypes = [_vp, _dp, ctypes.c_uint32, ctypes.c_int]
+        L.ref_cells_accelerate.argtypes = [_vp, _dp, ctypes.c_uint32, ctypes.c_int]
+        L.ref_cells_moments.argtypes = [_vp, ctypes.c_uint32, _dp, _dp, _dp]
+        L.ref_bailouts.restype = ctypes.c_int
+
+    def init(self, mesh: VelocityMesh, wall_margin: int = 1):
+        vmin = np.array(mesh.vmin, np.float64)
+        vmax = np.array(mesh.vmax, np.float64)
+        ln = np.array(mesh.length, np.uint32)
+        self.lib.ref_init(_ptr(vmin, ctypes.c_double), _ptr(vmax, ctypes.c_double), _ptr(ln, ctypes.c_uint32),
+                          wall_margin)
+
+    def create(self, gid_list, data_list, min_values):
+        offs = np.zeros(len(gid_list) + 1, np.uint64)
+        offs[1:] = np.cumsum([len(g) for g in gid_list])
+        gids = np.ascontiguousarray(np.concatenate(gid_list).astype(np.uint32))
+        data = np.ascontiguousarray(np.concatenate([d.reshape(-1, WID3) for d in data_list]).astype(self.realf))
+        mv = np.ascontiguousarray(np.asarray(min_values, np.float64))
+        return self.lib.ref_cells_create(len(gid_list), _ptr(offs, ctypes.c_uint64), _ptr(gids, ctypes.c_uint32),
+                                         _ptr(data, self._ct), _ptr(mv, ctypes.c_double))
+
+    def destroy(self, h):
+        self.lib.ref_cells_destroy(h)
+
+    def extract(self, h, c, sort=True):
+        n = self.lib.ref_cells_block_count(h, c)
+        g = np.zeros(max(n, 1), np.uint32)
+        d = np.zeros((max(n, 1), WID3), self.realf)
+        self.lib.ref_cells_extract(h, c, _ptr(g, ctypes.c_uint32), _ptr(d, self._ct), n)
+        g, d = g[:n], d[:n]
+        if sort:
+            o = np.argsort(g, kind="stable")
+            g, d = g[o], d[o]
+        return g, d
+
+    def map_1d(self, h, isect, dim, nthreads=0):
+        isect = np.ascontiguousarray(isect, np.float64)
+        self.lib.ref_cells_map_1d(h, _ptr(isect, ctypes.c_double), dim, nthreads)
+
+    def accelerate(self, h, isect12, map_order, nthreads=0):
+        isect12 = np.ascontiguousarray(isect12, np.float64)
+        self.lib.ref_cells_accelerate(h, _ptr(isect12, ctypes.c_double), map_order, nthreads)
+
+    def moments(self, h, c, bulk_v):
+        bv = np.ascontiguousarray(bulk_v, np.float64)
+        f = np.zeros(4)
+        s = np.zeros(6)
+        self.lib.ref_cells_moments(h, c, _ptr(bv, ctypes.c_double), _ptr(f, ctypes.c_double),
+                                   _ptr(s, ctypes.c_double))
+        return f, s
+
+    def bailouts(self) -> int:
+        return self.lib.ref_bailouts()

@@ -1,0 +1,167 @@
+// C entry points over the reference's own CPU acceleration code, used as the
+// parity oracle and CPU baseline (test infrastructure only; built by
+// oracle/build_ref.sh into oracle/_ref/, never linked into the product).
+//
+// The functions below build shim SpatialCells from flat (GID, data) arrays,
+// call the reference's map_1d (vlasovsolver/cpu_acc_map.cpp:121-636) exactly
+// as cpu_accelerate_cell does (vlasovsolver/cpu_acc_semilag.cpp:92-130), and
+// read the resulting blocks back out.  The moment sums call the reference's
+// blockVelocityFirstMoments / blockVelocitySecondMoments templates
+// (vlasovsolver/arch_moments.h:83-155).
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+#include "memoryallocation.h"
+#include "object_wrapper.h"
+#include "vlasovsolver/cpu_acc_map.hpp"
+#include "vlasovsolver/arch_moments.h"
+
+using spatial_cell::SpatialCell;
+
+uint Parameters::bailout_velocity_space_wall_margin = 1;
+Real Parameters::maxSlAccelerationRotation = 25.0;
+Real Parameters::hallMinimumRhoq = 1.602176634e-19;
+uint Parameters::ohmGradPeTerm = 0;
+bool Parameters::prepareForRebalance = false;
+uint Parameters::tstep = 0;
+
+static ObjectWrapper g_objects;
+ObjectWrapper& getObjectWrapper() { return g_objects; }
+
+// The reference raises a global bail-out flag on fatal conditions
+// (common.cpp:36-95); here every bail-out is counted so the caller can see it.
+static int g_bailouts = 0;
+void bailout(const bool condition, const std::string&, const char* const, const int) {
+   if (condition) {
+#pragma omp atomic
+      g_bailouts++;
+   }
+}
+void bailout(const bool condition, const std::string& m) { bailout(condition, m, "", 0); }
+void bailout(const bool condition, const char* const f, const int l) { bailout(condition, "", f, l); }
+void memory_purge() {}
+
+static bool g_mesh_ready = false;
+
+extern "C" {
+
+int ref_realf_size() { return (int)sizeof(Realf); }
+
+// One velocity mesh: limits in m/s, grid length in blocks, WID cells per block.
+int ref_init(const double vmin[3], const double vmax[3], const uint32_t grid_length[3], uint32_t wall_margin) {
+   if (!g_mesh_ready) {
+      vmesh::allocateMeshWrapper();
+      vmesh::MeshParameters mp;
+      mp.name = "mesh0";
+      for (int d = 0; d < 3; ++d) {
+         mp.meshLimits[2 * d] = vmin[d];
+         mp.meshLimits[2 * d + 1] = vmax[d];
+         mp.gridLength[d] = grid_length[d];
+         mp.blockLength[d] = WID;
+      }
+      vmesh::host_getMeshWrapper()->velocityMeshesCreation->push_back(mp);
+      vmesh::host_getMeshWrapper()->initVelocityMeshes(1);
+      g_objects.particleSpecies.resize(1);
+      g_mesh_ready = true;
+   }
+   Parameters::bailout_velocity_space_wall_margin = wall_margin;
+   return 0;
+}
+
+int ref_bailouts() { return g_bailouts; }
+void ref_reset_bailouts() { g_bailouts = 0; }
+
+// ---- a set of cells kept alive across calls (for timing without set-up) ----
+struct RefCells {
+   std::vector<SpatialCell*> cells;
+};
+
+void* ref_cells_create(uint32_t n_cells, const uint64_t* offsets, const uint32_t* gids, const Realf* data,
+                       const double* min_values) {
+   RefCells* rc = new RefCells();
+   rc->cells.resize(n_cells);
+#pragma omp parallel for schedule(dynamic, 16)
+   for (uint32_t c = 0; c < n_cells; ++c) {
+      SpatialCell* sc = new SpatialCell(1);
+      sc->get_velocity_mesh(0)->initialize(0);
+      sc->populations[0]->velocityBlockMinValue = min_values[c];
+      sc->parameters[CellParams::CELLID] = c + 1;
+      const uint64_t b0 = offsets[c], b1 = offsets[c + 1];
+      for (uint64_t b = b0; b < b1; ++b) {
+         if (!sc->add_velocity_block(gids[b], 0)) continue;
+         const vmesh::LocalID lid = sc->get_velocity_mesh(0)->getLocalID(gids[b]);
+         std::memcpy(sc->get_velocity_blocks(0)->getData(lid), data + b * WID3, sizeof(Realf) * WID3);
+      }
+      rc->cells[c] = sc;
+   }
+   return rc;
+}
+
+void ref_cells_destroy(void* h) {
+   RefCells* rc = (RefCells*)h;
+   for (auto* c : rc->cells) delete c;
+   delete rc;
+}
+
+uint64_t ref_cells_block_count(void* h, uint32_t c) { return ((RefCells*)h)->cells[c]->get_velocity_mesh(0)->size(); }
+
+// Copies cell c's blocks out in the container's local-ID order.
+uint64_t ref_cells_extract(void* h, uint32_t c, uint32_t* gids, Realf* data, uint64_t cap) {
+   SpatialCell* sc = ((RefCells*)h)->cells[c];
+   const uint64_t n = sc->get_velocity_mesh(0)->size();
+   if (n > cap) return n;
+   for (uint64_t lid = 0; lid < n; ++lid) {
+      gids[lid] = sc->get_velocity_mesh(0)->getGlobalID(lid);
+      std::memcpy(data + lid * WID3, sc->get_velocity_blocks(0)->getData(lid), sizeof(Realf) * WID3);
+   }
+   return n;
+}
+
+// One 1D sweep on every cell: intersections holds 4 doubles per cell
+// (intersection, di, dj, dk) for this dimension.
+void ref_cells_map_1d(void* h, const double* intersections, uint32_t dimension, int nthreads) {
+   RefCells* rc = (RefCells*)h;
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      const double* I = intersections + 4 * c;
+      map_1d(rc->cells[c], 0, I[0], I[1], I[2], I[3], dimension);
+   }
+}
+
+// Three sweeps per cell in map_order 0 (XYZ), 1 (YZX) or 2 (ZXY), as
+// cpu_accelerate_cell does; intersections holds 12 doubles per cell ordered
+// x(4), y(4), z(4).
+void ref_cells_accelerate(void* h, const double* intersections, uint32_t map_order, int nthreads) {
+   RefCells* rc = (RefCells*)h;
+   static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      const double* I = intersections + 12 * c;
+      for (int s = 0; s < 3; ++s) {
+         const uint32_t d = orders[map_order % 3][s];
+         map_1d(rc->cells[c], 0, I[4 * d + 0], I[4 * d + 1], I[4 * d + 2], I[4 * d + 3], d);
+      }
+   }
+}
+
+// First moments (n, nVx, nVy, nVz) and, about the given bulk velocity, the
+// six second moments of cell c, with the reference's own reduction templates.
+void ref_cells_moments(void* h, uint32_t c, const double* bulk_v, double* first4, double* second6) {
+   SpatialCell* sc = ((RefCells*)h)->cells[c];
+   const uint n = sc->get_velocity_mesh(0)->size();
+   Real a1[4] = {0, 0, 0, 0};
+   Real a2[6] = {0, 0, 0, 0, 0, 0};
+   if (n > 0) {
+      blockVelocityFirstMoments(sc->get_velocity_blocks(0), a1, n);
+      blockVelocitySecondMoments(sc->get_velocity_blocks(0), (Real)bulk_v[0], (Real)bulk_v[1], (Real)bulk_v[2], a2, n);
+   }
+   for (int i = 0; i < 4; ++i) first4[i] = a1[i];
+   for (int i = 0; i < 6; ++i) second6[i] = a2[i];
+}
+
+}  // extern "C"
