@@ -1,0 +1,186 @@
+/*
+ * vlgpu.h -- C ABI of the B200 Vlasov hot path (libvlgpu.so).
+ *
+ * The entry points act on a device-resident batch of spatial cells, each
+ * holding one population's sparse velocity mesh: a list of velocity-block
+ * global IDs (GID = i + j*Nx + k*Nx*Ny) and 64 Realf (float) values per
+ * block, x fastest.  They replace, for that data, the reference's
+ * per-cell CPU functions listed beside each declaration (paths relative to
+ * the Vlasiator source tree).  Plain pointers and sizes only; all calls
+ * return a VLGPU_* status code.  A batch belongs to one host thread at a time.
+ */
+#ifndef VLGPU_H
+#define VLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Per-cell conditions are also reported bitwise through
+   vlgpu_batch_status (VLGPU_CELL_*). */
+#define VLGPU_OK 0
+#define VLGPU_EINVAL 1    /* bad argument */
+#define VLGPU_ENOMEM 2    /* device allocation failed or a pool is full */
+#define VLGPU_EWALL 3     /* some target block came within the wall margin (reference bail-out, cpu_acc_map.cpp:325-338) */
+#define VLGPU_ETIMEDOUT 4 /* a bounded device-side wait gave up */
+#define VLGPU_ERANGE 5    /* a column's target window exceeded the remap ring (rotation per step too large) */
+#define VLGPU_ECUDA 6     /* CUDA runtime error */
+#define VLGPU_ENODEV 7    /* no CUDA device */
+
+#define VLGPU_CELL_WALL 1u
+#define VLGPU_CELL_RANGE 2u
+#define VLGPU_CELL_NOMEM 4u
+#define VLGPU_CELL_BADDK 8u
+
+/* Velocity mesh: vmesh::MeshParameters (velocity_mesh_parameters.h:53).
+   len = blocks per axis (<= 96); WID = 4 cells per block per axis. */
+typedef struct vlgpu_mesh {
+   double vmin[3];
+   double vmax[3];
+   uint32_t len[3];
+} vlgpu_mesh;
+
+/* Species and solver settings read by the hot path
+   (object_wrapper.cpp:44-68,111-145; parameters.cpp:392-493). */
+typedef struct vlgpu_params {
+   double charge;            /* C */
+   double mass;              /* kg */
+   double min_value;         /* <pop>_sparse.minValue */
+   uint32_t add_width_v;     /* <pop>_sparse.blockAddWidthV */
+   uint32_t wall_margin;     /* bailout.velocity_space_wall_block_margin */
+   double hall_minimum_rhoq; /* Parameters::hallMinimumRhoq */
+   uint32_t ohm_gradpe;      /* fieldsolver.ohmGradPeTerm */
+   uint32_t reserved;
+} vlgpu_params;
+
+/* Per-cell field inputs of the acceleration transform, as read from
+   SpatialCell::parameters / derivativesBVOL (cpu_acc_transform.cpp:71-89). */
+typedef struct vlgpu_cell_fields {
+   double B[3];       /* BGB?VOL + PERB?VOL */
+   double curl[3];    /* (dBZdy - dBYdz, dBXdz - dBZdx, dBYdx - dBXdy) of the perturbed field */
+   double egradpe[3]; /* E?GRADPE; RHOQ_V and V_V come from the cell's own moments */
+} vlgpu_cell_fields;
+
+typedef struct vlgpu_batch vlgpu_batch;
+
+/* ---- batch life cycle ---------------------------------------------------- */
+
+/* Creates a batch of n_cells cells on `device` with room for block_capacity
+   blocks per pool (two pools are kept for out-of-place sweeps). */
+int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint32_t n_cells, uint64_t block_capacity,
+                       int device, vlgpu_batch** out);
+int vlgpu_batch_destroy(vlgpu_batch* b);
+
+/* Host -> device: cell c owns blocks offsets[c] .. offsets[c+1]-1 of gids /
+   data (64 floats per block).  Replaces the blocks of every cell and clears
+   the per-cell status. */
+int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* gids, const float* data);
+
+/* Number of blocks per cell (n_cells entries). */
+int vlgpu_batch_block_counts(vlgpu_batch* b, uint32_t* counts);
+
+/* Device -> host: blocks of every cell, ascending GID within a cell, packed
+   by cell; offsets has n_cells+1 entries; capacity in blocks. */
+int vlgpu_batch_download(vlgpu_batch* b, uint64_t* offsets, uint32_t* gids, float* data, uint64_t capacity);
+
+/* Device -> host without reordering: the pool holding the current state is
+   copied verbatim up to its highest used block (*used blocks); cell c owns
+   blocks cell_off[c] .. cell_off[c]+cell_count[c]-1 of it, in the sweep's
+   output order (like the reference's local-ID order, not sorted). */
+int vlgpu_batch_download_raw(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
+                             uint64_t capacity, uint64_t* used);
+
+/* Per-cell VLGPU_CELL_* bits accumulated since the last upload. */
+int vlgpu_batch_status(vlgpu_batch* b, uint32_t* status);
+
+/* ---- the hot path ------------------------------------------------------- */
+
+/* One SLICE-3D 1D remap along `dimension` of every cell of the batch.
+   Replaces map_1d (vlasovsolver/cpu_acc_map.hpp:30-32, cpu_acc_map.cpp:121-636)
+   called once per cell.  intersections: 4 doubles per cell (intersection,
+   di, dj, dk) in host memory, as stored in Population::intersection_*
+   (spatial_cell_cpu.hpp:89-92). */
+int vlgpu_map_1d(vlgpu_batch* b, const double* intersections, uint32_t dimension);
+
+/* The same sweep issued as one launch sequence per cell (the plain per-cell
+   drop-in path, vlasovsolver/cpu_acc_semilag.cpp:64-75 without OpenMP). */
+int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t dimension);
+
+/* Three sweeps in map_order 0 (XYZ), 1 (YZX) or 2 (ZXY) with given
+   intersections (12 doubles per cell ordered x, y, z; cpu_accelerate_cell,
+   vlasovsolver/cpu_acc_semilag.cpp:92-130). */
+int vlgpu_accelerate_with_intersections(vlgpu_batch* b, const double* intersections12, uint32_t map_order);
+
+/* One acceleration step of every cell, as calculateAcceleration does for
+   one population and one subcycle (vlasovsolver/vlasovmover.cpp:410-475,
+   564-569): first velocity moments of the current VDF give the pivot
+   (calculateMoments_V), the FP64 gyration transform and intersections are
+   built per cell on the device (cpu_acc_transform.cpp:66-153,
+   cpu_acc_intersections.cpp:44-450), the three sweeps run in map_order, the
+   blocks are adjusted (adjustVelocityBlocks, grid.cpp:775-817, cells without
+   spatial neighbours) and the moments including the pressure tensor are
+   recomputed.  fields: one vlgpu_cell_fields per cell; dt: one substep length
+   per cell (Population::subcycleDt); host memory. */
+int vlgpu_accelerate(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt, uint32_t map_order);
+
+/* The same step reusing the fields and dt last passed to vlgpu_accelerate
+   (no host data; suitable for stream capture). */
+int vlgpu_accelerate_device(vlgpu_batch* b, uint32_t map_order);
+
+/* The same step with every sweep issued as one launch sequence per cell: the
+   plain per-cell path, kept as the drop-in baseline of the batched one. */
+int vlgpu_accelerate_per_cell(vlgpu_batch* b, uint32_t map_order);
+
+/* Block adjustment of every cell (SpatialCell::adjust_velocity_blocks,
+   spatial_cells/spatial_cell_cpu.cpp:179-273, no spatial neighbours):
+   keeps the blocks with content and their +-blockAddWidthV velocity
+   neighbours, removes the rest, adds missing neighbours with zero data. */
+int vlgpu_adjust_blocks(vlgpu_batch* b);
+
+/* Mass removed by block adjustment per cell since the last upload
+   (Population::RHOLOSSADJUST, sum f dv^3). */
+int vlgpu_batch_rho_loss(vlgpu_batch* b, double* out);
+
+/* Velocity moments of every cell's current VDF (calculateMoments_V,
+   vlasovsolver/arch_moments.cpp:342-499, one population), FP64 with
+   compensated sums.  The record of the last vlgpu_accelerate holds the
+   post-step moments already; this call recomputes them.  out16: 16 doubles per cell: n, n*V (3), RHOM_V, V_V (3),
+   RHOQ_V, P_11, P_22, P_33, P_23, P_13, P_12 (zero unless compute_second),
+   sum of f. */
+int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16);
+
+/* The 12 FP64 intersections per cell (x, y, z; each intersection, di, dj,
+   dk) computed by the last vlgpu_accelerate. */
+int vlgpu_batch_intersections(vlgpu_batch* b, double* out12);
+
+/* The CUDA stream (cudaStream_t) all of the batch's work is issued on, for
+   callers that time it with events or order their own work after it. */
+int vlgpu_batch_stream(vlgpu_batch* b, void** stream);
+
+/* Enables (1) or disables (0) CUDA-event timing of every remap launch and
+   clears the accumulated time. */
+int vlgpu_batch_profile(vlgpu_batch* b, int enable);
+
+/* Counters since creation: [0] kernels launched, [1] cell-sweeps,
+   [2] source blocks entering sweeps, [3] blocks written by sweeps,
+   [4] remap launches, [5] profiled remap time (ns), [6] profiled remap
+   launches, [7] column sets remapped.  Synchronises the stream. */
+int vlgpu_batch_stats(vlgpu_batch* b, uint64_t* out8);
+
+/* Further counters: [0] blocks that entered the first sweep of each
+   acceleration step (the step's phase-space cell updates / 64). */
+int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out);
+
+/* Synchronises the batch's stream and returns the first error seen. */
+int vlgpu_batch_sync(vlgpu_batch* b);
+
+/* Library version string. */
+const char* vlgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VLGPU_H */

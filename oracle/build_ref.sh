@@ -48,6 +48,10 @@ COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
 SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
       "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
       "$SRC/velocity_mesh_parameters.cpp")
-"$CXX" "${COMMON[@]}" -DSPF -DVECL=16 "${SRCS[@]}" -o "$OUT/libvlasov_ref_sp.so"
-"$CXX" "${COMMON[@]}" -DDPF -DVECL=8 "${SRCS[@]}" -o "$OUT/libvlasov_ref_dp.so"
+# the oracle's own FP64 geometry restatement (the reference's needs Eigen)
+CC="${REF_CC:-/usr/bin/gcc}"
+"$CC" -O2 -std=c11 -fPIC -ffp-contract=off -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_sp.o"
+"$CC" -O2 -std=c11 -fPIC -ffp-contract=off -DORC_DOUBLE -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_dp.o"
+"$CXX" "${COMMON[@]}" -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" -o "$OUT/libvlasov_ref_sp.so"
+"$CXX" "${COMMON[@]}" -DDPF -DVECL=8 "${SRCS[@]}" "$OUT/orc_geometry_dp.o" -o "$OUT/libvlasov_ref_dp.so"
 echo "build_ref: built $OUT/libvlasov_ref_sp.so $OUT/libvlasov_ref_dp.so"

@@ -57,6 +57,12 @@ class Restatement:
                                                  ctypes.c_double, _dp, _dp]
         L.orc_cell_intersections.restype = None
         L.orc_cell_intersections.argtypes = [_dp, _dp, ctypes.POINTER(CMesh), ctypes.c_uint32, _dp]
+        L.orc_moments.restype = None
+        L.orc_moments.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_adjust.restype = ctypes.c_int
+        L.orc_adjust.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, ctypes.POINTER(ct), _dp]
 
     def map_1d(self, mesh: VelocityMesh, gids, data, isect4, dim: int, min_value: float, wall_margin: int = 1,
                cap: int | None = None):
@@ -75,6 +81,49 @@ class Restatement:
         if rc != 0:
             raise RuntimeError(f"orc_map_1d failed with status {rc}")
         return go[: n.value].copy(), do[: n.value].copy(), fl.value
+
+    def moments(self, mesh: VelocityMesh, gids, data, mass, charge, second=True):
+        gids = np.ascontiguousarray(gids, dtype=np.uint32)
+        data = np.ascontiguousarray(data, dtype=self.realf).reshape(-1, WID3)
+        out = np.zeros(16)
+        cm = CMesh.of(mesh)
+        self.lib.orc_moments(ctypes.byref(cm), len(gids), _ptr(gids, ctypes.c_uint32), _ptr(data, self._ct),
+                             float(mass), float(charge), int(second), _ptr(out, ctypes.c_double))
+        return out
+
+    def adjust(self, mesh: VelocityMesh, gids, data, min_value, add_width=1):
+        gids = np.ascontiguousarray(gids, dtype=np.uint32)
+        data = np.ascontiguousarray(data, dtype=self.realf).reshape(-1, WID3)
+        cap = max(30 * len(gids) + 64, 1024)
+        go = np.zeros(cap, np.uint32)
+        do = np.zeros((cap, WID3), self.realf)
+        n = ctypes.c_uint32(0)
+        loss = ctypes.c_double(0)
+        cm = CMesh.of(mesh)
+        rc = self.lib.orc_adjust(ctypes.byref(cm), len(gids), _ptr(gids, ctypes.c_uint32), _ptr(data, self._ct),
+                                 float(min_value), int(add_width), cap, ctypes.byref(n), _ptr(go, ctypes.c_uint32),
+                                 _ptr(do, self._ct), ctypes.byref(loss))
+        if rc != 0:
+            raise RuntimeError(f"orc_adjust failed with status {rc}")
+        return go[: n.value].copy(), do[: n.value].copy(), loss.value
+
+    def accelerate_step(self, mesh: VelocityMesh, gids, data, B, dt, map_order, mass, charge, min_value=1e-15,
+                        add_width=1, hall_min_rhoq=1.60217653e-19, mu0=1.25663706e-6):
+        """One acceleration step of one cell as the reference's calculateAcceleration
+        does it for one subcycle: moments -> transform -> intersections -> three
+        map_1d -> block adjustment -> moments with pressure."""
+        m0 = self.moments(mesh, gids, data, mass, charge, second=False)
+        L, t = self.acceleration_transform(B, np.zeros(3), m0[8], m0[5:8], np.zeros(3), charge, mass, dt,
+                                           hall_min_rhoq, 0, mu0)
+        isect = self.cell_intersections(L, t, mesh, map_order)
+        g, d = gids, data
+        wall = 0
+        for dim in [[0, 1, 2], [1, 2, 0], [2, 0, 1]][map_order]:
+            g, d, fl = self.map_1d(mesh, g, d, isect[4 * dim:4 * dim + 4], dim, min_value)
+            wall |= fl
+        g, d, loss = self.adjust(mesh, g, d, min_value, add_width)
+        m1 = self.moments(mesh, g, d, mass, charge, second=True)
+        return g, d, isect, loss, m1, wall
 
     def acceleration_transform(self, B, curl, rhoq, V, egradpe, q, m, dt, hall_min_rhoq, ohm_gradpe, mu0):
         L = np.zeros(9)
@@ -127,6 +176,9 @@ class ReferenceBuild:
         L.ref_cells_accelerate.argtypes = [_vp, _dp, ctypes.c_uint32, ctypes.c_int]
         L.ref_cells_moments.argtypes = [_vp, ctypes.c_uint32, _dp, _dp, _dp]
         L.ref_bailouts.restype = ctypes.c_int
+        L.ref_cells_accelerate_step.argtypes = [_vp, _dp, _dp, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_int]
+        L.ref_max_threads.restype = ctypes.c_int
 
     def init(self, mesh: VelocityMesh, wall_margin: int = 1):
         vmin = np.array(mesh.vmin, np.float64)
@@ -165,6 +217,15 @@ class ReferenceBuild:
     def accelerate(self, h, isect12, map_order, nthreads=0):
         isect12 = np.ascontiguousarray(isect12, np.float64)
         self.lib.ref_cells_accelerate(h, _ptr(isect12, ctypes.c_double), map_order, nthreads)
+
+    def accelerate_step(self, h, B, dt, map_order, charge, mass, nthreads=0):
+        B = np.ascontiguousarray(B, np.float64)
+        dt = np.ascontiguousarray(dt, np.float64)
+        self.lib.ref_cells_accelerate_step(h, _ptr(B, ctypes.c_double), _ptr(dt, ctypes.c_double), map_order,
+                                           charge, mass, nthreads)
+
+    def max_threads(self) -> int:
+        return self.lib.ref_max_threads()
 
     def moments(self, h, c, bulk_v):
         bv = np.ascontiguousarray(bulk_v, np.float64)

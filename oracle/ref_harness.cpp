@@ -23,7 +23,7 @@ using spatial_cell::SpatialCell;
 
 uint Parameters::bailout_velocity_space_wall_margin = 1;
 Real Parameters::maxSlAccelerationRotation = 25.0;
-Real Parameters::hallMinimumRhoq = 1.602176634e-19;
+Real Parameters::hallMinimumRhoq = 1.60217653e-19;
 uint Parameters::ohmGradPeTerm = 0;
 bool Parameters::prepareForRebalance = false;
 uint Parameters::tstep = 0;
@@ -163,5 +163,58 @@ void ref_cells_moments(void* h, uint32_t c, const double* bulk_v, double* first4
    for (int i = 0; i < 4; ++i) first4[i] = a1[i];
    for (int i = 0; i < 6; ++i) second6[i] = a2[i];
 }
+
+// One acceleration step per cell, the body of calculateAcceleration for one
+// substep (vlasovsolver/vlasovmover.cpp:410-475) without the block
+// adjustment: first moments with the reference's reduction template give the
+// pivot velocity (calculateMoments_V), the FP64 transform and intersections
+// come from the oracle's restatement (the reference needs Eigen for them), and
+// the reference's map_1d runs three times in map_order.  B: 3 doubles per cell;
+// dt: one per cell.
+void orc_acceleration_transform(const double B[3], const double curl_terms[3], double rhoq_v, const double V[3],
+                                const double egradpe[3], double q, double m, double dt, double hall_min_rhoq,
+                                int ohm_gradpe, double mu0, double out_L[9], double out_t[3]);
+struct orc_mesh_c {
+   double vmin[3];
+   double vmax[3];
+   uint32_t len[3];
+};
+void orc_cell_intersections(const double fwd_L[9], const double fwd_t[3], const orc_mesh_c* m, uint32_t map_order,
+                            double out12[12]);
+
+void ref_cells_accelerate_step(void* h, const double* B, const double* dt, uint32_t map_order, double charge,
+                               double mass, int nthreads) {
+   RefCells* rc = (RefCells*)h;
+   static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+   const vmesh::MeshParameters& mp = (*vmesh::host_getMeshWrapper()->velocityMeshes)[0];
+   orc_mesh_c om;
+   for (int d = 0; d < 3; ++d) {
+      om.vmin[d] = mp.meshMinLimits[d];
+      om.vmax[d] = mp.meshMaxLimits[d];
+      om.len[d] = mp.gridLength[d];
+   }
+#pragma omp parallel for schedule(dynamic, 1)
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      SpatialCell* sc = rc->cells[c];
+      const uint n = sc->get_velocity_mesh(0)->size();
+      Real a[4] = {0, 0, 0, 0};
+      if (n > 0) blockVelocityFirstMoments(sc->get_velocity_blocks(0), a, n);
+      const double rhom = a[0] * mass;
+      const double V[3] = {rhom != 0 ? (a[1] * mass) / rhom : 0.0, rhom != 0 ? (a[2] * mass) / rhom : 0.0,
+                           rhom != 0 ? (a[3] * mass) / rhom : 0.0};
+      const double zero[3] = {0, 0, 0};
+      double L[9], t[3], I[12];
+      orc_acceleration_transform(B + 3 * c, zero, a[0] * charge, V, zero, charge, mass, dt[c],
+                                 Parameters::hallMinimumRhoq, 0, 1.25663706e-6, L, t);
+      orc_cell_intersections(L, t, &om, map_order % 3, I);
+      for (int s = 0; s < 3; ++s) {
+         const uint32_t d = orders[map_order % 3][s];
+         map_1d(sc, 0, I[4 * d + 0], I[4 * d + 1], I[4 * d + 2], I[4 * d + 3], d);
+      }
+   }
+}
+
+int ref_max_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"

@@ -615,3 +615,123 @@ void orc_cell_intersections(const double fwd_L[9], const double fwd_t[3], const 
    isect_2nd(&bwd, mn, dv, o[1], out12 + 4 * o[1]);
    isect_3rd(&bwd, mn, dv, o[2], out12 + 4 * o[2]);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Velocity moments of one cell, vlasovsolver/arch_moments.h:83-155 and the   */
+/* per-population bookkeeping of calculateMoments_V                           */
+/* (vlasovsolver/arch_moments.cpp:342-499).  out16: n, n*V(3), RHOM_V, V(3),  */
+/* RHOQ_V, P_11, P_22, P_33, P_23, P_13, P_12, sum f.  Plain sums in double,  */
+/* blocks in the given order, cells i fastest.                                */
+/* ------------------------------------------------------------------------- */
+void orc_moments(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf* data, double mass, double charge,
+                 int second, double out16[16]) {
+   const double bs[3] = {(m->vmax[0] - m->vmin[0]) / m->len[0], (m->vmax[1] - m->vmin[1]) / m->len[1],
+                         (m->vmax[2] - m->vmin[2]) / m->len[2]};
+   const double dv[3] = {bs[0] / WID, bs[1] / WID, bs[2] / WID};
+   const double DV3 = dv[0] * dv[1] * dv[2];
+   double a[5] = {0, 0, 0, 0, 0};
+   for (uint32_t b = 0; b < n; ++b) {
+      const uint32_t g = gids[b];
+      const uint32_t bi = g % m->len[0], bj = (g / m->len[0]) % m->len[1], bk = g / (m->len[0] * m->len[1]);
+      for (int c = 0; c < WID3; ++c) {
+         const int i = c % WID, j = (c / WID) % WID, k = c / WID2;
+         const double VX = (m->vmin[0] + bi * bs[0]) + (i + 0.5) * dv[0];
+         const double VY = (m->vmin[1] + bj * bs[1]) + (j + 0.5) * dv[1];
+         const double VZ = (m->vmin[2] + bk * bs[2]) + (k + 0.5) * dv[2];
+         const double f = (double)data[(size_t)b * WID3 + c];
+         a[0] += f * DV3;
+         a[1] += f * VX * DV3;
+         a[2] += f * VY * DV3;
+         a[3] += f * VZ * DV3;
+         a[4] += f;
+      }
+   }
+   for (int q = 0; q < 16; ++q) out16[q] = 0.0;
+   out16[0] = a[0]; out16[1] = a[1]; out16[2] = a[2]; out16[3] = a[3];
+   const double rhom = a[0] * mass;
+   out16[4] = rhom;
+   out16[5] = rhom != 0.0 ? (a[1] * mass) / rhom : 0.0;
+   out16[6] = rhom != 0.0 ? (a[2] * mass) / rhom : 0.0;
+   out16[7] = rhom != 0.0 ? (a[3] * mass) / rhom : 0.0;
+   out16[8] = a[0] * charge;
+   out16[15] = a[4];
+   if (!second) return;
+   const double V[3] = {out16[5], out16[6], out16[7]};
+   double p[6] = {0, 0, 0, 0, 0, 0};
+   for (uint32_t b = 0; b < n; ++b) {
+      const uint32_t g = gids[b];
+      const uint32_t bi = g % m->len[0], bj = (g / m->len[0]) % m->len[1], bk = g / (m->len[0] * m->len[1]);
+      for (int c = 0; c < WID3; ++c) {
+         const int i = c % WID, j = (c / WID) % WID, k = c / WID2;
+         const double VX = (m->vmin[0] + bi * bs[0]) + (i + 0.5) * dv[0];
+         const double VY = (m->vmin[1] + bj * bs[1]) + (j + 0.5) * dv[1];
+         const double VZ = (m->vmin[2] + bk * bs[2]) + (k + 0.5) * dv[2];
+         const double f = (double)data[(size_t)b * WID3 + c];
+         p[0] += f * (VX - V[0]) * (VX - V[0]) * DV3;
+         p[1] += f * (VY - V[1]) * (VY - V[1]) * DV3;
+         p[2] += f * (VZ - V[2]) * (VZ - V[2]) * DV3;
+         p[3] += f * (VY - V[1]) * (VZ - V[2]) * DV3;
+         p[4] += f * (VX - V[0]) * (VZ - V[2]) * DV3;
+         p[5] += f * (VX - V[0]) * (VY - V[1]) * DV3;
+      }
+   }
+   for (int q = 0; q < 6; ++q) out16[9 + q] = mass * p[q];
+}
+
+/* ------------------------------------------------------------------------- */
+/* Block adjustment of one cell without spatial neighbours,                  */
+/* SpatialCell::adjust_velocity_blocks (spatial_cells/spatial_cell_cpu.cpp:  */
+/* 179-273) with the content test of compute_block_has_content (:290-320):   */
+/* the new set is the content blocks and their +-add_width neighbours inside */
+/* the mesh; kept blocks keep their data, added ones are zero, the removed   */
+/* mass sum(f)*dv^3 is returned in *loss.  Output sorted by global ID.        */
+/* ------------------------------------------------------------------------- */
+int orc_adjust(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf* data, double min_value,
+               int add_width, uint32_t cap, uint32_t* n_out, uint32_t* gids_out, realf* data_out, double* loss) {
+   const uint32_t L0 = m->len[0], L1 = m->len[1], L2 = m->len[2];
+   const size_t nb = (size_t)L0 * L1 * L2;
+   int32_t* where = (int32_t*)malloc(sizeof(int32_t) * nb);
+   unsigned char* keep = (unsigned char*)calloc(nb, 1);
+   if (!where || !keep) { free(where); free(keep); return ORC_ENOMEM; }
+   for (size_t q = 0; q < nb; ++q) where[q] = -1;
+   for (uint32_t b = 0; b < n; ++b) where[gids[b]] = (int32_t)b;
+   for (uint32_t b = 0; b < n; ++b) {
+      int content = 0;
+      for (int c = 0; c < WID3; ++c)
+         if ((double)data[(size_t)b * WID3 + c] >= min_value) { content = 1; break; }
+      if (!content) continue;
+      const int x = (int)(gids[b] % L0), y = (int)((gids[b] / L0) % L1), z = (int)(gids[b] / (L0 * L1));
+      for (int dx = -add_width; dx <= add_width; ++dx)
+         for (int dy = -add_width; dy <= add_width; ++dy)
+            for (int dz = -add_width; dz <= add_width; ++dz) {
+               const int X = x + dx, Y = y + dy, Z = z + dz;
+               if (X < 0 || Y < 0 || Z < 0 || X >= (int)L0 || Y >= (int)L1 || Z >= (int)L2) continue;
+               keep[(size_t)X + L0 * ((size_t)Y + L1 * (size_t)Z)] = 1;
+            }
+   }
+   const double dvx = (m->vmax[0] - m->vmin[0]) / L0 / WID, dvy = (m->vmax[1] - m->vmin[1]) / L1 / WID,
+                dvz = (m->vmax[2] - m->vmin[2]) / L2 / WID;
+   const double DV3 = dvx * dvy * dvz;
+   double lost = 0.0;
+   for (uint32_t b = 0; b < n; ++b) {
+      if (keep[gids[b]]) continue;
+      double sum = 0.0;
+      for (int c = 0; c < WID3; ++c) sum += data[(size_t)b * WID3 + c];
+      lost += DV3 * sum;
+   }
+   uint32_t o = 0;
+   int status = ORC_OK;
+   for (size_t g = 0; g < nb; ++g) {
+      if (!keep[g]) continue;
+      if (o >= cap) { status = ORC_ENOMEM; break; }
+      gids_out[o] = (uint32_t)g;
+      if (where[g] >= 0) memcpy(data_out + (size_t)o * WID3, data + (size_t)where[g] * WID3, sizeof(realf) * WID3);
+      else memset(data_out + (size_t)o * WID3, 0, sizeof(realf) * WID3);
+      ++o;
+   }
+   *n_out = o;
+   *loss = lost;
+   free(where);
+   free(keep);
+   return status;
+}

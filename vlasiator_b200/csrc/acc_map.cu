@@ -1,0 +1,647 @@
+// SLICE-3D one-dimensional acceleration remap on sparse 4x4x4 velocity blocks
+// for sm_100a.  One sweep is two kernels:
+//
+//   columnize_kernel  one CTA per cell.  Builds the cell's column structure
+//                     for the sweep dimension from 96-bit occupancy masks in
+//                     shared memory (one mask per transverse block pair),
+//                     computes each column's target block range with the
+//                     reference's rule (cpu_acc_map.cpp:258-324), allocates
+//                     the cell's output blocks and writes one ColumnSet record
+//                     per transverse pair plus the source permutation.
+//
+//   remap_kernel      persistent; each half-warp takes one ColumnSet and
+//                     walks it along the sweep dimension, one lane per
+//                     transverse cell (i,j) of the 4x4 block face.  PPM
+//                     coefficients are built in registers from a sliding
+//                     5-cell window; each source cell's mass is distributed
+//                     over the Lagrangian target cells it overlaps into a
+//                     per-lane ring of 8 target blocks in shared memory, and
+//                     completed target blocks are streamed out.  Every output
+//                     block is written exactly once, so no zero fill and no
+//                     atomics are needed.
+//
+// Arithmetic follows the reference's scalar build operation by operation
+// (round-to-nearest intrinsics, no contraction, the double-precision
+// products of cpu_face_estimates.hpp:163 and cpu_acc_map.cpp:585), so results
+// are bit-identical to the reference's map_1d on the same inputs.
+#include <cfloat>
+#include <cstdint>
+
+#include "vlgpu_common.cuh"
+
+namespace vlgpu {
+
+// ---------------------------------------------------------------------------
+// exact IEEE single-precision helpers (never contracted into FMA)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
+// double constant times float, rounded once to float (VecSimple<float> * double)
+__device__ __forceinline__ float dmf(double c, float x) { return __double2float_rn(__dmul_rn(c, (double)x)); }
+
+// h4 left face value, cpu_face_estimates.hpp:160-167
+__device__ __forceinline__ float h4_face(float vm2, float vm1, float v0, float vp1) {
+   float s = fa(-vm2, fm(7.0f, vm1));
+   s = fa(s, fm(7.0f, v0));
+   s = fs(s, vp1);
+   return dmf(1.0 / 12.0, s);
+}
+
+__device__ __forceinline__ float minmod(float s1, float s2) {
+   const float slope = (fabsf(s1) < fabsf(s2)) ? s1 : s2;
+   return (fm(s1, s2) <= 0.0f) ? 0.0f : slope;
+}
+__device__ __forceinline__ float maxmod(float s1, float s2) {
+   const float slope = (fabsf(s1) > fabsf(s2)) ? s1 : s2;
+   return (fm(s1, s2) <= 0.0f) ? 0.0f : slope;
+}
+
+// PPM coefficients of cpu_1d_ppm.hpp:35-54 (filtered h4 faces, superbee,
+// Colella-Woodward monotonicity) for the cell with neighbours vm1, vp1 and
+// raw faces fl (left) / fr (right).
+__device__ __forceinline__ void ppm_coeff(float vm1, float v0, float vp1, float fl, float fr, float threshold,
+                                          float scale, float& a0, float& a1, float& a2) {
+   const float l = fm(vm1, scale), m = fm(v0, scale), r = fm(vp1, scale);
+   const float a = fs(r, m), b = fs(m, l);
+   const float s1 = minmod(a, fm(2.0f, b));
+   const float s2 = minmod(fm(2.0f, a), b);
+   const float slope = maxmod(s1, s2);
+   const float slope_abs = fm(fabsf(slope), threshold);
+   const float slope_sign = (slope > 0.0f) ? 1.0f : -1.0f;
+   if (slope_abs == 0.0f) {
+      fr = v0;
+      fl = v0;
+   }
+   const float half_slope = fm(fm(slope_sign, 0.5f), slope_abs);
+   if (fm(fs(vm1, fl), fs(fl, v0)) < 0.0f) fl = fs(v0, half_slope);
+   if (fm(fs(vp1, fr), fs(fr, v0)) < 0.0f) fr = fa(v0, half_slope);
+   const float one_sixth = (float)(1.0 / 6.0);
+   {
+      const float d = fs(fr, fl);
+      const float e = fs(v0, fm(0.5f, fa(fl, fr)));
+      if (fm(d, e) > fm(fm(d, d), one_sixth)) fl = fs(fm(3.0f, v0), fm(2.0f, fr));
+   }
+   {
+      const float d = fs(fr, fl);
+      const float e = fs(v0, fm(0.5f, fa(fl, fr)));
+      if (fm(fm(-d, d), one_sixth) > fm(d, e)) fr = fs(fm(3.0f, v0), fm(2.0f, fl));
+   }
+   a0 = fl;
+   a1 = fs(fs(fm(3.0f, v0), fm(2.0f, fl)), fr);
+   a2 = fs(fa(fl, fr), fm(2.0f, v0));
+}
+
+// ---------------------------------------------------------------------------
+// 96-bit mask helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int mask_next_set(const uint32_t m[3], int k) {
+   for (; k < 96; k = (k | 31) + 1) {
+      const uint32_t w = m[k >> 5] >> (k & 31);
+      if (w) return k + __ffs(w) - 1;
+   }
+   return 96;
+}
+__device__ __forceinline__ int mask_next_clear(const uint32_t m[3], int k) {
+   for (; k < 96; k = (k | 31) + 1) {
+      const uint32_t w = (~m[k >> 5]) >> (k & 31);
+      if (w) return k + __ffs(w) - 1;
+   }
+   return 96;
+}
+
+// Target block range of one column (cpu_acc_map.cpp:307-338).  Returns true
+// when the range violates the wall margin.
+__device__ __forceinline__ bool column_extent(float mx, float mn, float dk, float dv, float v_min, int max_len,
+                                              int first_k, int last_k, int wall_margin, int& fb, int& lb) {
+   const float first_min_v = fa(fm((float)(WID * first_k), dv), v_min);
+   const float last_max_v = fa(fm((float)(WID * (last_k + 1)), dv), v_min);
+   const int first_gk = __float2int_rz(fd(fs(first_min_v, mx), dk));
+   const int last_gk = __float2int_rz(fd(fs(last_max_v, mn), dk));
+   fb = first_gk / WID;
+   lb = last_gk / WID;
+   fb = (fb >= 0) ? fb : 0;
+   fb = (fb < max_len) ? fb : max_len - 1;
+   lb = (lb >= 0) ? lb : 0;
+   lb = (lb < max_len) ? lb : max_len - 1;
+   return fb < wall_margin || fb >= max_len - wall_margin || lb < wall_margin || lb >= max_len - wall_margin;
+}
+
+// The set's corner extremes of the Lagrangian starting point
+// (cpu_acc_map.cpp:258-288), evaluated exactly as the reference does.
+__device__ __forceinline__ void set_corners(const SweepCell& P, uint32_t si, uint32_t sj, float& mx, float& mn) {
+   const float A0 = (float)(si * WID), A1 = (float)(si * WID + WID - 1);
+   const float B0 = (float)(sj * WID), B1 = (float)(sj * WID + WID - 1);
+   const float c00 = fa(fa(P.intersection, fm(A0, P.di)), fm(B0, P.dj));
+   const float c01 = fa(fa(P.intersection, fm(A0, P.di)), fm(B1, P.dj));
+   const float c10 = fa(fa(P.intersection, fm(A1, P.di)), fm(B0, P.dj));
+   const float c11 = fa(fa(P.intersection, fm(A1, P.di)), fm(B1, P.dj));
+   mx = c00;
+   mx = (mx < c01) ? c01 : mx;
+   mx = (mx < c10) ? c10 : mx;
+   mx = (mx < c11) ? c11 : mx;
+   mn = c00;
+   mn = (c01 < mn) ? c01 : mn;
+   mn = (c10 < mn) ? c10 : mn;
+   mn = (c11 < mn) ? c11 : mn;
+}
+
+// ---------------------------------------------------------------------------
+// columnize: one CTA per cell
+// ---------------------------------------------------------------------------
+constexpr int COL_THREADS = 512;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   uint32_t x = v;
+#pragma unroll
+   for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+   }
+   if (lane == 31) warp_sums[warp] = x;
+   __syncthreads();
+   if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      uint32_t s = (lane < nw) ? warp_sums[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+         const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+         if (lane >= o) s += y;
+      }
+      if (lane < nw) warp_sums[lane] = s;
+   }
+   __syncthreads();
+   total = warp_sums[(blockDim.x >> 5) - 1];
+   const uint32_t before = (warp > 0) ? warp_sums[warp - 1] : 0u;
+   __syncthreads();
+   return before + x - v;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ src_slots,
+   CellSlot* __restrict__ dst_slots, uint32_t* __restrict__ perm, ColumnSet* __restrict__ sets,
+   uint32_t set_capacity, uint32_t dst_capacity,
+   const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
+   BatchStats* __restrict__ stats, MeshDev mesh, int wall_margin, uint32_t cell_begin, uint32_t cell_end,
+   int first_of_step) {
+   extern __shared__ uint32_t smem[];
+   __shared__ uint32_t warp_sums[32];
+   __shared__ uint32_t s_bbox[4];
+   __shared__ uint32_t s_set_base, s_dst_base, s_nsets, s_ntgt, s_flags;
+
+   const uint32_t cell = cell_begin + blockIdx.x;
+   if (cell >= cell_end) return;
+   const CellSlot src = src_slots[cell];
+   const SweepCell P = sweep_cells[cell];
+   uint32_t li, lj;
+   plane_lengths(mesh.len, DIM, li, lj);
+   const int max_len = (int)mesh.len[DIM];
+
+   if (threadIdx.x == 0) {
+      s_bbox[0] = 0xffffffffu; s_bbox[1] = 0; s_bbox[2] = 0xffffffffu; s_bbox[3] = 0;
+      s_flags = 0;
+   }
+   __syncthreads();
+   if (src.count == 0) {
+      if (threadIdx.x == 0) dst_slots[cell] = CellSlot{0u, 0u};
+      return;
+   }
+   // pass 1: bounding box of the transverse indices
+   {
+      uint32_t a0 = 0xffffffffu, a1 = 0, b0 = 0xffffffffu, b1 = 0;
+      for (uint32_t b = threadIdx.x; b < src.count; b += blockDim.x) {
+         uint32_t s[3];
+         swapped_indices(gids[src.off + b], mesh.len, DIM, s);
+         a0 = min(a0, s[0]); a1 = max(a1, s[0]);
+         b0 = min(b0, s[1]); b1 = max(b1, s[1]);
+      }
+      atomicMin(&s_bbox[0], a0); atomicMax(&s_bbox[1], a1);
+      atomicMin(&s_bbox[2], b0); atomicMax(&s_bbox[3], b1);
+   }
+   __syncthreads();
+   const uint32_t a_lo = s_bbox[0], b_lo = s_bbox[2];
+   const uint32_t na = s_bbox[1] - a_lo + 1, nb = s_bbox[3] - b_lo + 1;
+   const uint32_t plane = na * nb;
+   uint32_t* mask = smem;                   // 3 * plane
+   uint32_t* prefix = smem + 3 * plane;     // plane
+   uint16_t* set_t = (uint16_t*)(prefix + plane);  // plane (set index -> t)
+   uint32_t* tcount = prefix + plane + (plane + 1) / 2;  // plane
+   for (uint32_t q = threadIdx.x; q < 3 * plane; q += blockDim.x) mask[q] = 0;
+   __syncthreads();
+   // pass 2: occupancy masks along the sweep dimension
+   for (uint32_t b = threadIdx.x; b < src.count; b += blockDim.x) {
+      uint32_t s[3];
+      swapped_indices(gids[src.off + b], mesh.len, DIM, s);
+      const uint32_t t = (s[0] - a_lo) * nb + (s[1] - b_lo);
+      atomicOr(&mask[3 * t + (s[2] >> 5)], 1u << (s[2] & 31));
+   }
+   __syncthreads();
+   // scan over the plane: source offsets and set indices
+   const uint32_t chunk = (plane + blockDim.x - 1) / blockDim.x;
+   const uint32_t t0 = min(plane, threadIdx.x * chunk), t1 = min(plane, t0 + chunk);
+   uint32_t my_blocks = 0, my_sets = 0;
+   for (uint32_t t = t0; t < t1; ++t) {
+      const uint32_t n = __popc(mask[3 * t]) + __popc(mask[3 * t + 1]) + __popc(mask[3 * t + 2]);
+      my_blocks += n;
+      my_sets += (n > 0);
+   }
+   uint32_t tot_blocks, tot_sets;
+   uint32_t blk_base = block_exclusive_scan(my_blocks, warp_sums, tot_blocks);
+   uint32_t set_base = block_exclusive_scan(my_sets, warp_sums, tot_sets);
+   for (uint32_t t = t0; t < t1; ++t) {
+      const uint32_t n = __popc(mask[3 * t]) + __popc(mask[3 * t + 1]) + __popc(mask[3 * t + 2]);
+      prefix[t] = blk_base;
+      blk_base += n;
+      if (n > 0) set_t[set_base++] = (uint16_t)t;
+   }
+   if (threadIdx.x == 0) {
+      const uint32_t base = atomicAdd(&counters->n_sets, tot_sets);
+      s_set_base = base;
+      s_nsets = tot_sets;
+      if (base + tot_sets > set_capacity) s_flags |= VLGPU_CELL_NOMEM;
+   }
+   __syncthreads();
+   const bool sets_ok = !(s_flags & VLGPU_CELL_NOMEM);
+   // per set: target mask from the column extents
+   uint32_t wall = 0, baddk = 0;
+   for (uint32_t s = threadIdx.x; s < tot_sets; s += blockDim.x) {
+      const uint32_t t = set_t[s];
+      const uint32_t si = a_lo + t / nb, sj = b_lo + t % nb;
+      uint32_t m[3] = {mask[3 * t], mask[3 * t + 1], mask[3 * t + 2]};
+      uint32_t tm[3] = {0u, 0u, 0u};
+      float mx, mn;
+      set_corners(P, si, sj, mx, mn);
+      if (!(P.dk > 0.0f)) baddk = 1;
+      int k = mask_next_set(m, 0);
+      while (k < 96) {
+         const int e = mask_next_clear(m, k) - 1;
+         int fb, lb;
+         if (column_extent(mx, mn, P.dk, mesh.dv[DIM], mesh.vmin[DIM], max_len, k, e, wall_margin, fb, lb)) wall = 1;
+         for (int q = fb; q <= lb; ++q) tm[q >> 5] |= 1u << (q & 31);
+         k = mask_next_set(m, e + 1);
+      }
+      tcount[s] = __popc(tm[0]) + __popc(tm[1]) + __popc(tm[2]);
+      if (sets_ok) {
+         ColumnSet cs;
+         cs.cell = cell;
+         cs.si = si;
+         cs.sj = sj;
+         cs.src_pos = src.off + prefix[t];
+         cs.dst_pos = 0;
+         cs.src_mask[0] = m[0]; cs.src_mask[1] = m[1]; cs.src_mask[2] = m[2];
+         cs.tgt_mask[0] = tm[0]; cs.tgt_mask[1] = tm[1]; cs.tgt_mask[2] = tm[2];
+         sets[s_set_base + s] = cs;
+      }
+   }
+   if (wall) atomicOr(&s_flags, VLGPU_CELL_WALL);
+   if (baddk) atomicOr(&s_flags, VLGPU_CELL_BADDK);
+   __syncthreads();
+   // scan of target counts over sets -> output positions
+   const uint32_t sch = (tot_sets + blockDim.x - 1) / blockDim.x;
+   const uint32_t q0 = min(tot_sets, threadIdx.x * sch), q1 = min(tot_sets, q0 + sch);
+   uint32_t my_t = 0;
+   for (uint32_t s = q0; s < q1; ++s) my_t += tcount[s];
+   uint32_t tot_t;
+   uint32_t tbase = block_exclusive_scan(my_t, warp_sums, tot_t);
+   if (threadIdx.x == 0) {
+      const uint32_t base = atomicAdd(&counters->dst_top, tot_t);
+      s_dst_base = base;
+      s_ntgt = tot_t;
+      if ((uint64_t)base + tot_t > dst_capacity) s_flags |= VLGPU_CELL_NOMEM;
+   }
+   __syncthreads();
+   const bool ok = !(s_flags & VLGPU_CELL_NOMEM);
+   if (ok) {
+      for (uint32_t s = q0; s < q1; ++s) {
+         sets[s_set_base + s].dst_pos = s_dst_base + tbase;
+         tbase += tcount[s];
+      }
+      // source permutation in (set, k) order
+      for (uint32_t b = threadIdx.x; b < src.count; b += blockDim.x) {
+         uint32_t s[3];
+         swapped_indices(gids[src.off + b], mesh.len, DIM, s);
+         const uint32_t t = (s[0] - a_lo) * nb + (s[1] - b_lo);
+         const uint32_t pos = prefix[t] + (uint32_t)mask_popc_below(&mask[3 * t], s[2]);
+         perm[src.off + pos] = src_index ? src_index[src.off + b] : src.off + b;
+      }
+   } else if (sets_ok) {
+      // no room for the output: neutralise this cell's sets
+      for (uint32_t s = threadIdx.x; s < tot_sets; s += blockDim.x) {
+         sets[s_set_base + s].tgt_mask[0] = 0;
+         sets[s_set_base + s].tgt_mask[1] = 0;
+         sets[s_set_base + s].tgt_mask[2] = 0;
+         sets[s_set_base + s].src_mask[0] = 0;
+         sets[s_set_base + s].src_mask[1] = 0;
+         sets[s_set_base + s].src_mask[2] = 0;
+      }
+   }
+   if (threadIdx.x == 0) {
+      atomicAdd(&stats->src_blocks, (unsigned long long)src.count);
+      atomicAdd(&stats->dst_blocks, (unsigned long long)(ok ? s_ntgt : 0u));
+      atomicAdd(&stats->sweeps, 1ull);
+      atomicAdd(&stats->sets, (unsigned long long)tot_sets);
+      if (first_of_step) atomicAdd(&stats->step_blocks, (unsigned long long)src.count);
+      dst_slots[cell] = ok ? CellSlot{s_dst_base, s_ntgt} : CellSlot{0u, 0u};
+      if (s_flags) atomicOr(&status[cell], s_flags);
+      if (!ok) atomicOr(&counters->overflow, 1u);
+   }
+}
+
+// Dynamic shared memory of columnize for a full transverse plane.
+size_t columnize_smem_bytes(uint32_t plane) {
+   return sizeof(uint32_t) * (3 * plane + plane + (plane + 1) / 2 + plane) + 16;
+}
+
+// ---------------------------------------------------------------------------
+// remap: persistent, one half-warp per column set
+// ---------------------------------------------------------------------------
+constexpr int REMAP_THREADS = 256;
+constexpr int RING_BLOCKS = 8;               // target blocks held per set
+constexpr int RING_CELLS = RING_BLOCKS * WID;  // per lane
+constexpr int RING_STRIDE = RING_CELLS * 16 + 16;  // floats per half-warp (+16 pad: bank shift)
+
+template <int DIM>
+__device__ __forceinline__ int cell_offset(int i, int j, int g) {
+   if (DIM == 0) return i * WID2 + j * WID + g;
+   if (DIM == 1) return i + j * WID2 + g * WID;
+   return i + j * WID + g * WID2;
+}
+
+constexpr uint32_t NO_BLOCK = 0xffffffffu;  // a block that exists with all-zero data
+
+template <int DIM>
+__device__ __forceinline__ void load_lane(const float* __restrict__ data, uint32_t idx, int i, int j, float v[4]) {
+   if (idx == NO_BLOCK) {
+      v[0] = v[1] = v[2] = v[3] = 0.0f;
+      return;
+   }
+   const float* __restrict__ blk = data + (size_t)idx * WID3;
+   if (DIM == 0) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(blk + cell_offset<0>(i, j, 0)));
+      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+   } else {
+#pragma unroll
+      for (int g = 0; g < 4; ++g) v[g] = __ldg(blk + cell_offset<DIM>(i, j, g));
+   }
+}
+
+template <int DIM>
+__device__ __forceinline__ void store_lane(float* __restrict__ blk, int i, int j, const float v[4]) {
+   if (DIM == 0) {
+      *reinterpret_cast<float4*>(blk + cell_offset<0>(i, j, 0)) = make_float4(v[0], v[1], v[2], v[3]);
+   } else {
+#pragma unroll
+      for (int g = 0; g < 4; ++g) blk[cell_offset<DIM>(i, j, g)] = v[g];
+   }
+}
+
+// Reference argmax / argmin lane selection (cpu_acc_map.cpp:515-529): the
+// first lane holding the largest value above DBL_MIN (default lane 0) and the
+// first lane holding the smallest value below DBL_MAX (default lane 0).
+__device__ __forceinline__ void select_lanes(float lag, int lane, unsigned hmask, int& max_lane, int& min_lane) {
+   bool vmax = (double)lag > DBL_MIN;
+   float xmax = lag;
+   int imax = lane;
+   bool vmin = (double)lag < DBL_MAX;
+   float xmin = lag;
+   int imin = lane;
+#pragma unroll
+   for (int o = 8; o >= 1; o >>= 1) {
+      const bool ov = __shfl_xor_sync(hmask, vmax, o, 16);
+      const float ox = __shfl_xor_sync(hmask, xmax, o, 16);
+      const int oi = __shfl_xor_sync(hmask, imax, o, 16);
+      if (ov && (!vmax || ox > xmax || (ox == xmax && oi < imax))) { vmax = true; xmax = ox; imax = oi; }
+      const bool nv = __shfl_xor_sync(hmask, vmin, o, 16);
+      const float nx = __shfl_xor_sync(hmask, xmin, o, 16);
+      const int ni = __shfl_xor_sync(hmask, imin, o, 16);
+      if (nv && (!vmin || nx < xmin || (nx == xmin && ni < imin))) { vmin = true; xmin = nx; imin = ni; }
+   }
+   max_lane = vmax ? imax : 0;
+   min_lane = vmin ? imin : 0;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
+   const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
+   const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
+   const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
+   uint32_t set_capacity, uint8_t* __restrict__ content_out, double content_threshold) {
+   __shared__ float ring_all[(REMAP_THREADS / 16) * RING_STRIDE];
+   const int hw = threadIdx.x >> 4;
+   const int lane = threadIdx.x & 15;
+   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+   float* ring = ring_all + hw * RING_STRIDE;
+   const int i = lane & 3, j = lane >> 2;
+   uint32_t n_sets = *((volatile uint32_t*)&counters->n_sets);
+   n_sets = (n_sets < set_capacity) ? n_sets : set_capacity;
+   const int max_len = (int)mesh.len[DIM];
+   const float dv = mesh.dv[DIM], v_min = mesh.vmin[DIM];
+   const double i_dv = 1.0 / (double)dv;
+
+   for (;;) {
+      uint32_t sidx = 0;
+      if (lane == 0) sidx = atomicAdd(&counters->work, 1u);
+      sidx = __shfl_sync(hmask, sidx, 0, 16);
+      if (sidx >= n_sets) break;
+      const ColumnSet cs = sets[sidx];
+      const SweepCell P = sweep_cells[cs.cell];
+      const float threshold = P.threshold;
+      const float scale = __double2float_rn(1.0 / (double)threshold);
+      const float dk = P.dk;
+      // lane's Lagrangian starting point (cpu_acc_map.cpp:493-496)
+      const float A = fa((float)(cs.si * WID), (float)i);
+      const float B = fa((float)(cs.sj * WID), (float)j);
+      const float im = fa(fa(P.intersection, fm(A, P.di)), fm(B, P.dj));
+      float mx, mn;
+      set_corners(P, cs.si, cs.sj, mx, mn);
+#pragma unroll
+      for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
+      int next_flush = mask_next_set(cs.tgt_mask, 0);
+      uint32_t out_idx = 0;
+      bool range_err = false;
+
+      // writes out every target block below `limit_block` that is still held
+      auto flush_until = [&](int limit_block) {
+         while (next_flush < 96 && next_flush < limit_block) {
+            float v[4];
+            const int slot = (next_flush & (RING_BLOCKS - 1)) * WID;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+               v[g] = ring[(slot + g) * 16 + lane];
+               ring[(slot + g) * 16 + lane] = 0.0f;
+            }
+            const uint32_t o = cs.dst_pos + out_idx;
+            store_lane<DIM>(dst_data + (size_t)o * WID3, i, j, v);
+            // content flag of the finished block (compute_block_has_content)
+            const bool c = ((double)v[0] >= content_threshold) | ((double)v[1] >= content_threshold) |
+                           ((double)v[2] >= content_threshold) | ((double)v[3] >= content_threshold);
+            const unsigned any_c = __ballot_sync(hmask, c) & hmask;
+            if (lane == 0) {
+               dst_gids[o] = gid_from_swapped(cs.si, cs.sj, (uint32_t)next_flush, mesh.len, DIM);
+               content_out[o] = any_c ? 1 : 0;
+            }
+            ++out_idx;
+            next_flush = mask_next_set(cs.tgt_mask, next_flush + 1);
+         }
+      };
+
+      int src_rank = 0;
+      int col_s = mask_next_set(cs.src_mask, 0);
+      int col_e = (col_s < 96) ? mask_next_clear(cs.src_mask, col_s) - 1 : 95;
+      int cf = 0, cl = 0;
+      if (col_s < 96) column_extent(mx, mn, dk, dv, v_min, max_len, col_s, col_e, wall_margin, cf, cl);
+      while (col_s < 96) {
+         const int nxt_s = mask_next_set(cs.src_mask, col_e + 1);
+         int nxt_e = 95, ncf = 1 << 20, ncl = 0;
+         if (nxt_s < 96) {
+            nxt_e = mask_next_clear(cs.src_mask, nxt_s) - 1;
+            column_extent(mx, mn, dk, dv, v_min, max_len, nxt_s, nxt_e, wall_margin, ncf, ncl);
+         }
+         // ---- map one column (cpu_acc_map.cpp:395-631) ----
+         float v_r = fa(fm((float)(WID * col_s), dv), v_min);
+         int gk_r;
+         int max_lane, min_lane;
+         {
+            const float lag = fd(fs(v_r, im), dk);
+            gk_r = __float2int_rz(lag);
+            select_lanes(lag, lane, hmask, max_lane, min_lane);
+         }
+         const int gk_lo_col = cf * WID, gk_hi_col = (cl + 1) * WID - 1;
+         float p2 = 0.0f, p1 = 0.0f;
+         float cur[4], nxt[4];
+         load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
+         if (col_e > col_s) {
+            load_lane<DIM>(src_data, perm[cs.src_pos + src_rank + 1], i, j, nxt);
+         } else {
+            nxt[0] = nxt[1] = nxt[2] = nxt[3] = 0.0f;
+         }
+         float face = h4_face(p2, p1, cur[0], cur[1]);
+         for (int kb = col_s; kb <= col_e; ++kb) {
+            float nn[4];
+            if (kb + 2 <= col_e) {
+               load_lane<DIM>(src_data, perm[cs.src_pos + src_rank + 2], i, j, nn);
+            } else {
+               nn[0] = nn[1] = nn[2] = nn[3] = 0.0f;
+            }
+            const float w[8] = {p2, p1, cur[0], cur[1], cur[2], cur[3], nxt[0], nxt[1]};
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+               const float fr = h4_face(w[g + 1], w[g + 2], w[g + 3], w[g + 4]);
+               float a0, a1, a2;
+               ppm_coeff(w[g + 1], w[g + 2], w[g + 3], face, fr, threshold, scale, a0, a1, a2);
+               face = fr;
+               const float v_l = v_r;
+               v_r = fa(v_r, dv);
+               const int gk_l = gk_r;
+               gk_r = __float2int_rz(fd(fs(v_r, im), dk));
+               int min_gk = __shfl_sync(hmask, gk_l, min_lane, 16);
+               int max_gk = __shfl_sync(hmask, gk_r, max_lane, 16);
+               min_gk = (min_gk > gk_lo_col) ? min_gk : gk_lo_col;
+               max_gk = (max_gk < gk_hi_col) ? max_gk : gk_hi_col;
+               if (max_gk >= min_gk) {
+                  if ((min_gk >> 2) < next_flush || (max_gk >> 2) >= next_flush + RING_BLOCKS) {
+                     range_err = true;
+                  } else {
+                     float dens_r = 0.0f;
+                     for (int gk = min_gk; gk <= max_gk; ++gk) {
+                        float x = fa(fm((float)(gk + 1), dk), im);
+                        x = (x > v_l) ? x : v_l;
+                        x = (x < v_r) ? x : v_r;
+                        const float u = __double2float_rn(__dmul_rn((double)fs(x, v_l), i_dv));
+                        const float dl = dens_r;
+                        dens_r = fm(u, fa(a0, fm(u, fa(a1, fm(u, a2)))));
+                        float* t = &ring[(gk & (RING_CELLS - 1)) * 16 + lane];
+                        *t = fa(*t, fs(dens_r, dl));
+                     }
+                  }
+               }
+            }
+            // targets below the next source cell's lower bound are complete
+            int lb = ncf * WID;
+            if (kb < col_e) {
+               int nl = __shfl_sync(hmask, gk_r, min_lane, 16);
+               nl = (nl > gk_lo_col) ? nl : gk_lo_col;
+               lb = (nl < lb) ? nl : lb;
+            }
+            flush_until(lb >> 2);
+            p2 = cur[2];
+            p1 = cur[3];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+               cur[g] = nxt[g];
+               nxt[g] = nn[g];
+            }
+            ++src_rank;
+         }
+         col_s = nxt_s;
+         col_e = nxt_e;
+         cf = ncf;
+         cl = ncl;
+      }
+      flush_until(1 << 20);
+      if (range_err && lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
+   }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch helpers (used by capi.cu)
+// ---------------------------------------------------------------------------
+cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_index, const CellSlot* src_slots,
+                             CellSlot* dst_slots,
+                             uint32_t* perm, ColumnSet* sets, uint32_t set_capacity, uint32_t dst_capacity,
+                             const SweepCell* sweep_cells, uint32_t* status, SweepCounters* counters,
+                             BatchStats* stats, const MeshDev& mesh, int wall_margin, uint32_t cell_begin,
+                             uint32_t cell_end, int first_of_step, cudaStream_t stream) {
+   uint32_t li, lj;
+   plane_lengths(mesh.len, dim, li, lj);
+   const size_t smem = columnize_smem_bytes(li * lj);
+   const uint32_t n = cell_end - cell_begin;
+   if (n == 0) return cudaSuccess;
+   cudaError_t e = cudaSuccess;
+#define VLGPU_COL(D)                                                                                             \
+   e = cudaFuncSetAttribute(columnize_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+   if (e != cudaSuccess) return e;                                                                              \
+   columnize_kernel<D><<<n, COL_THREADS, smem, stream>>>(gids, src_index, src_slots, dst_slots, perm, sets,      \
+                                                         set_capacity,                                          \
+                                                         dst_capacity, sweep_cells, status, counters, stats, mesh, \
+                                                         wall_margin, cell_begin, cell_end, first_of_step);
+   if (dim == 0) { VLGPU_COL(0) } else if (dim == 1) { VLGPU_COL(1) } else { VLGPU_COL(2) }
+#undef VLGPU_COL
+   return cudaGetLastError();
+}
+
+cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
+                         const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
+                         uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
+                         uint8_t* content_out, double content_threshold, int grid, cudaStream_t stream) {
+   if (dim == 0)
+      remap_kernel<0><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
+                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
+   else if (dim == 1)
+      remap_kernel<1><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
+                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
+   else
+      remap_kernel<2><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
+                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
+   return cudaGetLastError();
+}
+
+// Points the remap work counter at the first set the next columnize launch
+// will create (per-cell launch sequences share one set array).
+__global__ void rebase_work_kernel(SweepCounters* counters) { counters->work = counters->n_sets; }
+
+cudaError_t launch_rebase_work(SweepCounters* counters, cudaStream_t stream) {
+   rebase_work_kernel<<<1, 1, 0, stream>>>(counters);
+   return cudaGetLastError();
+}
+
+int remap_blocks_per_sm() {
+   int n = 0;
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2>, REMAP_THREADS, 0);
+   return n > 0 ? n : 1;
+}
+
+}  // namespace vlgpu

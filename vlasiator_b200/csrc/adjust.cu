@@ -1,0 +1,289 @@
+// Sparse velocity-block adjustment for sm_100a.
+//
+// Semantics of SpatialCell::adjust_velocity_blocks
+// (spatial_cells/spatial_cell_cpu.cpp:179-273) for cells without spatial
+// neighbours: the new block set is H = the blocks with content (any cell >=
+// minValue, compute_block_has_content, spatial_cell_cpu.cpp:290-320) dilated
+// by +-blockAddWidthV in all three velocity directions, clipped to the mesh.
+// Blocks with content always stay, blocks in H keep their data, blocks not
+// in H are removed and their mass sum(f)*dv^3 is added to RHOLOSSADJUST,
+// blocks of H that did not exist are added with zero data.
+//
+// One CTA per cell.  The content set and H live in shared memory as 96-bit
+// x-masks over the (y,z) rows of the cell's dilated bounding box.  The output
+// is a new block list sorted by global ID plus, per block, the index of its
+// data in the current pool (or none for an added block): no VDF value is
+// copied, the next sweep reads the kept blocks where they are.
+#include <cstdint>
+
+#include "vlgpu_common.cuh"
+
+namespace vlgpu {
+
+constexpr int ADJ_THREADS = 512;
+constexpr uint32_t NO_BLOCK = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t adj_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   uint32_t x = v;
+#pragma unroll
+   for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+   }
+   if (lane == 31) warp_sums[warp] = x;
+   __syncthreads();
+   if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      uint32_t s = (lane < nw) ? warp_sums[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+         const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+         if (lane >= o) s += y;
+      }
+      if (lane < nw) warp_sums[lane] = s;
+   }
+   __syncthreads();
+   total = warp_sums[(blockDim.x >> 5) - 1];
+   const uint32_t before = (warp > 0) ? warp_sums[warp - 1] : 0u;
+   __syncthreads();
+   return before + x - v;
+}
+
+// Content of one block: any of its 64 values >= min_value (compared in
+// double, as the reference compares Realf data with the Real threshold).
+__device__ __forceinline__ bool block_has_content(const float* __restrict__ blk, double min_value) {
+   const float4* q = reinterpret_cast<const float4*>(blk);
+   bool c = false;
+   for (int i = 0; i < 16; ++i) {
+      const float4 v = __ldg(q + i);
+      c |= ((double)v.x >= min_value) | ((double)v.y >= min_value) | ((double)v.z >= min_value) |
+           ((double)v.w >= min_value);
+   }
+   return c;
+}
+
+__device__ __forceinline__ uint32_t shl96(uint32_t w0, uint32_t w1, uint32_t w2, int word, int s) {
+   // word `word` of the 96-bit value (w0,w1,w2) shifted left by s (0 <= s < 32)
+   if (s == 0) return word == 0 ? w0 : (word == 1 ? w1 : w2);
+   if (word == 0) return w0 << s;
+   if (word == 1) return (w1 << s) | (w0 >> (32 - s));
+   return (w2 << s) | (w1 >> (32 - s));
+}
+__device__ __forceinline__ uint32_t shr96(uint32_t w0, uint32_t w1, uint32_t w2, int word, int s) {
+   if (s == 0) return word == 0 ? w0 : (word == 1 ? w1 : w2);
+   if (word == 0) return (w0 >> s) | (w1 << (32 - s));
+   if (word == 1) return (w1 >> s) | (w2 << (32 - s));
+   return w2 >> s;
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
+   const uint8_t* __restrict__ content, const float* __restrict__ data, uint32_t* __restrict__ out_gids,
+   uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots, double* __restrict__ loss,
+   uint32_t* __restrict__ status, SweepCounters* __restrict__ counters, uint32_t out_capacity, MeshDev mesh,
+   double min_value, int add_width, double dv3) {
+   extern __shared__ uint32_t smem[];
+   __shared__ uint32_t warp_sums[32];
+   __shared__ int s_box[4];
+   __shared__ uint32_t s_base, s_flags;
+   __shared__ double s_loss[ADJ_THREADS / 32];
+
+   const uint32_t cell = blockIdx.x;
+   const CellSlot s = slots[cell];
+   const uint32_t L0 = mesh.len[0], L1 = mesh.len[1], L2 = mesh.len[2];
+   if (threadIdx.x == 0) {
+      s_box[0] = 1 << 20; s_box[1] = -1; s_box[2] = 1 << 20; s_box[3] = -1;
+      s_flags = 0;
+   }
+   __syncthreads();
+   // pass 1: bounding box (y, z) of the content blocks
+   {
+      int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
+      for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+         const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
+         bool c;
+         if (idx == NO_BLOCK) c = false;
+         else if (content) c = content[s.off + b] != 0;
+         else c = block_has_content(data + (size_t)idx * WID3, min_value);
+         if (c) {
+            const uint32_t g = gids[s.off + b];
+            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+            y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
+         }
+      }
+      atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
+      atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
+   }
+   __syncthreads();
+   const bool any = s_box[1] >= 0;
+   const int y0 = any ? max(0, s_box[0] - add_width) : 0;
+   const int y1 = any ? min((int)L1 - 1, s_box[1] + add_width) : -1;
+   const int z0 = any ? max(0, s_box[2] - add_width) : 0;
+   const int z1 = any ? min((int)L2 - 1, s_box[3] + add_width) : -1;
+   const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+   const uint32_t rows = any ? (uint32_t)(ny * nz) : 0u;
+   uint32_t* C = smem;              // 3 * rows
+   uint32_t* H = smem + 3 * rows;   // 3 * rows
+   uint32_t* prefix = smem + 6 * rows;  // rows
+   for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) C[q] = 0;
+   __syncthreads();
+   // pass 2: content mask rows
+   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
+      bool c;
+      if (idx == NO_BLOCK) c = false;
+      else if (content) c = content[s.off + b] != 0;
+      else c = block_has_content(data + (size_t)idx * WID3, min_value);
+      if (c) {
+         const uint32_t g = gids[s.off + b];
+         const uint32_t x = g % L0;
+         const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+         const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+         atomicOr(&C[3 * r + (x >> 5)], 1u << (x & 31));
+      }
+   }
+   __syncthreads();
+   // dilation: H(y,z) = OR over |dy|,|dz| <= w of the row dilated along x
+   const uint32_t xmask2 = (L0 >= 96) ? 0xffffffffu : ((L0 <= 64) ? 0u : ((1u << (L0 - 64)) - 1u));
+   const uint32_t xmask1 = (L0 >= 64) ? 0xffffffffu : ((L0 <= 32) ? 0u : ((1u << (L0 - 32)) - 1u));
+   const uint32_t xmask0 = (L0 >= 32) ? 0xffffffffu : ((1u << L0) - 1u);
+   uint32_t my_count = 0;
+   const uint32_t chunk = (rows + blockDim.x - 1) / blockDim.x;
+   const uint32_t r0 = min(rows, threadIdx.x * chunk), r1 = min(rows, r0 + chunk);
+   for (uint32_t r = r0; r < r1; ++r) {
+      const int yy = y0 + (int)(r % ny), zz = z0 + (int)(r / ny);
+      uint32_t h0 = 0, h1 = 0, h2 = 0;
+      for (int dz = -add_width; dz <= add_width; ++dz) {
+         const int z = zz + dz;
+         if (z < z0 || z > z1) continue;
+         for (int dy = -add_width; dy <= add_width; ++dy) {
+            const int y = yy + dy;
+            if (y < y0 || y > y1) continue;
+            const uint32_t rr = (uint32_t)((z - z0) * ny + (y - y0));
+            const uint32_t c0 = C[3 * rr], c1 = C[3 * rr + 1], c2 = C[3 * rr + 2];
+            h0 |= c0; h1 |= c1; h2 |= c2;
+            for (int sft = 1; sft <= add_width; ++sft) {
+               h0 |= shl96(c0, c1, c2, 0, sft) | shr96(c0, c1, c2, 0, sft);
+               h1 |= shl96(c0, c1, c2, 1, sft) | shr96(c0, c1, c2, 1, sft);
+               h2 |= shl96(c0, c1, c2, 2, sft) | shr96(c0, c1, c2, 2, sft);
+            }
+         }
+      }
+      h0 &= xmask0; h1 &= xmask1; h2 &= xmask2;
+      H[3 * r] = h0; H[3 * r + 1] = h1; H[3 * r + 2] = h2;
+      my_count += __popc(h0) + __popc(h1) + __popc(h2);
+   }
+   uint32_t total;
+   uint32_t base_r = adj_exclusive_scan(my_count, warp_sums, total);
+   for (uint32_t r = r0; r < r1; ++r) {
+      prefix[r] = base_r;
+      base_r += __popc(H[3 * r]) + __popc(H[3 * r + 1]) + __popc(H[3 * r + 2]);
+   }
+   if (threadIdx.x == 0) {
+      const uint32_t base = atomicAdd(&counters->dst_top, total);
+      s_base = base;
+      if ((uint64_t)base + total > out_capacity) s_flags |= VLGPU_CELL_NOMEM;
+   }
+   __syncthreads();
+   const bool ok = !(s_flags & VLGPU_CELL_NOMEM);
+   if (ok) {
+      // emit the new list in global-ID order; data indices default to "added"
+      for (uint32_t r = r0; r < r1; ++r) {
+         const uint32_t yy = (uint32_t)(y0 + (int)(r % ny)), zz = (uint32_t)(z0 + (int)(r / ny));
+         uint32_t o = s_base + prefix[r];
+         for (int w = 0; w < 3; ++w) {
+            uint32_t m = H[3 * r + w];
+            while (m) {
+               const int bit = __ffs(m) - 1;
+               m &= m - 1;
+               const uint32_t x = (uint32_t)(w * 32 + bit);
+               out_gids[o] = x + L0 * (yy + L1 * zz);
+               out_src[o] = NO_BLOCK;
+               ++o;
+            }
+         }
+      }
+   }
+   __syncthreads();
+   // old blocks: kept ones point the new entry at their data, removed ones
+   // feed the density loss
+   double lsum = 0.0;
+   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+      const uint32_t g = gids[s.off + b];
+      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
+      const uint32_t x = g % L0;
+      const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+      bool inH = false;
+      uint32_t pos = 0;
+      if (any && y >= y0 && y <= y1 && z >= z0 && z <= z1) {
+         const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+         inH = (H[3 * r + (x >> 5)] >> (x & 31)) & 1u;
+         pos = prefix[r] + (uint32_t)mask_popc_below(&H[3 * r], x);
+      }
+      if (inH) {
+         if (ok) out_src[s_base + pos] = idx;
+      } else if (idx != NO_BLOCK) {
+         const float* blk = data + (size_t)idx * WID3;
+         double sum = 0.0;
+         for (int q = 0; q < WID3; ++q) sum += (double)blk[q];
+         lsum += dv3 * sum;
+      }
+   }
+   // CTA sum of the removed mass
+#pragma unroll
+   for (int o = 16; o >= 1; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+   if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = lsum;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < ADJ_THREADS / 32; ++w) t += s_loss[w];
+      loss[cell] += t;
+      out_slots[cell] = ok ? CellSlot{s_base, total} : CellSlot{0u, 0u};
+      if (s_flags) atomicOr(&status[cell], s_flags);
+      if (!ok) atomicOr(&counters->overflow, 1u);
+   }
+}
+
+size_t adjust_smem_bytes(const MeshDev& mesh) { return sizeof(uint32_t) * 7 * mesh.len[1] * mesh.len[2] + 16; }
+
+cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const CellSlot* slots,
+                          const uint8_t* content, const float* data, uint32_t* out_gids, uint32_t* out_src,
+                          CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
+                          uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
+                          uint32_t n_cells, cudaStream_t stream) {
+   if (n_cells == 0) return cudaSuccess;
+   const size_t smem = adjust_smem_bytes(mesh);
+   cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+   if (e != cudaSuccess) return e;
+   adjust_kernel<<<n_cells, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, out_gids, out_src,
+                                                          out_slots, loss, status, counters, out_capacity, mesh,
+                                                          min_value, add_width, dv3);
+   return cudaGetLastError();
+}
+
+}  // namespace vlgpu
+
+namespace vlgpu {
+
+// dst row p = src row src_index[p] (zeros for an added block), p < n_blocks
+__global__ void materialize_kernel(const uint32_t* __restrict__ src_index, const float4* __restrict__ src,
+                                   float4* __restrict__ dst, uint64_t n_blocks) {
+   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   const uint64_t p = t >> 4;
+   const int q = (int)(t & 15);
+   if (p >= n_blocks) return;
+   const uint32_t idx = src_index[p];
+   dst[p * 16 + q] = (idx == NO_BLOCK) ? make_float4(0.f, 0.f, 0.f, 0.f) : src[(uint64_t)idx * 16 + q];
+}
+
+cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
+                               cudaStream_t stream) {
+   if (n_blocks == 0) return cudaSuccess;
+   const uint64_t threads = n_blocks * 16;
+   materialize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(
+      src_index, reinterpret_cast<const float4*>(src), reinterpret_cast<float4*>(dst), n_blocks);
+   return cudaGetLastError();
+}
+
+}  // namespace vlgpu

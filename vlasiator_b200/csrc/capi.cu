@@ -1,0 +1,629 @@
+// C ABI of libvlgpu.so: device-resident cell batches and the hot-path entry
+// points declared in include/vlgpu.h.
+//
+// A batch's VDF state is a block list per cell (global IDs, slot = offset and
+// count into the list) plus, optionally, a per-block index into the data pool
+// that holds the values.  Sweeps are out of place between two data pools and
+// leave a direct state (block b of a cell is data row off+b).  Block
+// adjustment leaves an indirect state (a new list whose entries point at the
+// kept rows, or at no row for added zero blocks), so it moves no VDF data.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "vlgpu_common.cuh"
+
+namespace vlgpu {
+cudaError_t launch_rebase_work(SweepCounters* counters, cudaStream_t stream);
+cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_index, const CellSlot* src_slots,
+                             CellSlot* dst_slots, uint32_t* perm, ColumnSet* sets, uint32_t set_capacity,
+                             uint32_t dst_capacity, const SweepCell* sweep_cells, uint32_t* status,
+                             SweepCounters* counters, BatchStats* stats, const MeshDev& mesh, int wall_margin,
+                             uint32_t cell_begin, uint32_t cell_end, int first_of_step, cudaStream_t stream);
+cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
+                         const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
+                         uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
+                         uint8_t* content_out, double content_threshold, int grid, cudaStream_t stream);
+int remap_blocks_per_sm();
+struct CellAccelInputs {
+   double B[3];
+   double curl[3];
+   double egradpe[3];
+   double dt;
+};
+cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
+                           double* moments, const MeshDev& mesh, const double vmin[3], const double bs[3],
+                           const double dv[3], double mass, double charge, bool second, uint32_t n_cells,
+                           cudaStream_t stream);
+cudaError_t launch_geometry(const CellAccelInputs* in, const double* moments, double* isect12, SweepCell* sweep3,
+                            uint32_t n_cells, double q, double m, double hall_min_rhoq, int ohm_gradpe, double mu0,
+                            const double vmin[3], const double dv[3], uint32_t map_order, float threshold,
+                            cudaStream_t stream);
+cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const CellSlot* slots,
+                          const uint8_t* content, const float* data, uint32_t* out_gids, uint32_t* out_src,
+                          CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
+                          uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
+                          uint32_t n_cells, cudaStream_t stream);
+cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
+                               cudaStream_t stream);
+constexpr int MOM_COUNT = 16;
+constexpr double MU_0 = 1.25663706e-6;  // physicalconstants::MU_0 (common.h:561)
+}  // namespace vlgpu
+
+using namespace vlgpu;
+
+struct vlgpu_batch {
+   int device = 0;
+   vlgpu_mesh mesh{};
+   vlgpu_params params{};
+   MeshDev mdev{};
+   uint32_t n_cells = 0;
+   uint64_t capacity = 0;  // blocks per pool
+   cudaStream_t stream = nullptr;
+   int sm_count = 0;
+   int remap_grid = 0;
+   double vmin_d[3], bs_d[3], dv_d[3];
+   // data pools and the lists written by sweeps into them
+   uint32_t* gids[2] = {nullptr, nullptr};
+   float* data[2] = {nullptr, nullptr};
+   CellSlot* slots[2] = {nullptr, nullptr};
+   uint8_t* content = nullptr;  // content flag per output row of the last sweep
+   // lists written by block adjustment (two, used alternately)
+   uint32_t* adj_gids[2] = {nullptr, nullptr};
+   uint32_t* adj_src[2] = {nullptr, nullptr};
+   CellSlot* adj_slots[2] = {nullptr, nullptr};
+   int adj_next = 0;
+   // the current state
+   const uint32_t* st_gids = nullptr;
+   const uint32_t* st_src = nullptr;  // null: direct
+   const CellSlot* st_slots = nullptr;
+   int cur = 0;                       // data pool holding the values
+   bool content_valid = false;        // content[] describes the current list
+   // work arrays
+   uint32_t* perm = nullptr;
+   ColumnSet* sets = nullptr;
+   SweepCell* sweep_cells = nullptr;
+   SweepCell* sweep3 = nullptr;  // 3 * n_cells, from the device geometry
+   CellAccelInputs* accel_in = nullptr;
+   double* moments = nullptr;  // MOM_COUNT per cell
+   double* isect12 = nullptr;  // 12 per cell
+   double* loss = nullptr;     // RHOLOSSADJUST per cell
+   uint32_t* status = nullptr;
+   SweepCounters* counters = nullptr;
+   BatchStats* stats = nullptr;
+   // pinned staging
+   SweepCell* h_sweep = nullptr;
+   CellAccelInputs* h_accel = nullptr;
+   // host-side accounting
+   unsigned long long launches = 0;
+   unsigned long long remap_launches = 0;
+   bool profiling = false;
+   std::vector<cudaEvent_t> prof_events;
+   size_t prof_used = 0;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e, const char* what) {
+   if (e == cudaSuccess) return VLGPU_OK;
+   std::fprintf(stderr, "vlgpu: %s: %s\n", what, cudaGetErrorString(e));
+   return e == cudaErrorMemoryAllocation ? VLGPU_ENOMEM : VLGPU_ECUDA;
+}
+
+#define VL_CHECK(call)                       \
+   do {                                      \
+      int _s = cuda_status((call), #call);   \
+      if (_s != VLGPU_OK) return _s;         \
+   } while (0)
+
+void free_batch(vlgpu_batch* b) {
+   if (!b) return;
+   cudaSetDevice(b->device);
+   for (int p = 0; p < 2; ++p) {
+      cudaFree(b->gids[p]);
+      cudaFree(b->data[p]);
+      cudaFree(b->slots[p]);
+      cudaFree(b->adj_gids[p]);
+      cudaFree(b->adj_src[p]);
+      cudaFree(b->adj_slots[p]);
+   }
+   cudaFree(b->content);
+   cudaFree(b->perm);
+   cudaFree(b->sets);
+   cudaFree(b->sweep_cells);
+   cudaFree(b->sweep3);
+   cudaFree(b->accel_in);
+   cudaFree(b->moments);
+   cudaFree(b->isect12);
+   cudaFree(b->loss);
+   cudaFree(b->status);
+   cudaFree(b->counters);
+   cudaFree(b->stats);
+   for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
+   cudaFreeHost(b->h_sweep);
+   cudaFreeHost(b->h_accel);
+   if (b->stream) cudaStreamDestroy(b->stream);
+   delete b;
+}
+
+// Per-cell sweep parameters in the swapped frame (cpu_acc_map.cpp:127-176).
+SweepCell make_sweep_cell(const double* I, uint32_t dim, double min_value) {
+   SweepCell s{};
+   float di = (float)I[1], dj = (float)I[2], dk = (float)I[3];
+   if (dim == 0) std::swap(di, dk);
+   if (dim == 1) std::swap(dj, dk);
+   s.intersection = (float)I[0];
+   s.di = di;
+   s.dj = dj;
+   s.dk = dk;
+   s.threshold = (float)min_value;
+   return s;
+}
+
+void set_direct_state(vlgpu_batch* b, int pool) {
+   b->st_gids = b->gids[pool];
+   b->st_src = nullptr;
+   b->st_slots = b->slots[pool];
+   b->cur = pool;
+}
+
+// One sweep of every cell; sweep parameters already on the device.
+int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, bool per_cell, bool first_of_step) {
+   const int src = b->cur, dst = 1 - b->cur;
+   const uint32_t cap = (uint32_t)b->capacity;
+   const int wm = (int)b->params.wall_margin;
+   const double thr = b->params.min_value;
+   VL_CHECK(cudaMemsetAsync(b->counters, 0, sizeof(SweepCounters), b->stream));
+   if (!per_cell) {
+      VL_CHECK(launch_columnize((int)dim, b->st_gids, b->st_src, b->st_slots, b->slots[dst], b->perm, b->sets, cap,
+                                cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm, 0, b->n_cells,
+                                first_of_step ? 1 : 0, b->stream));
+      const bool prof = b->profiling && b->prof_used + 2 <= b->prof_events.size();
+      if (prof) VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used], b->stream));
+      VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
+                            sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->remap_grid, b->stream));
+      if (prof) {
+         VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used + 1], b->stream));
+         b->prof_used += 2;
+      }
+      b->launches += 2;
+      b->remap_launches += 1;
+   } else {
+      // one columnize + remap launch pair per cell; set and output counters
+      // keep running so the cells land in disjoint ranges
+      for (uint32_t c = 0; c < b->n_cells; ++c) {
+         VL_CHECK(launch_rebase_work(b->counters, b->stream));
+         VL_CHECK(launch_columnize((int)dim, b->st_gids, b->st_src, b->st_slots, b->slots[dst], b->perm, b->sets,
+                                   cap, cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm, c, c + 1,
+                                   first_of_step ? 1 : 0, b->stream));
+         VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
+                               sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->sm_count, b->stream));
+         b->launches += 3;
+         b->remap_launches += 1;
+      }
+   }
+   set_direct_state(b, dst);
+   b->content_valid = true;
+   return VLGPU_OK;
+}
+
+// One sweep with host-given intersections (4 doubles per cell at `stride`).
+int run_sweep(vlgpu_batch* b, const double* intersections, size_t stride, uint32_t dim, bool per_cell) {
+   for (uint32_t c = 0; c < b->n_cells; ++c)
+      b->h_sweep[c] = make_sweep_cell(intersections + stride * c, dim, b->params.min_value);
+   VL_CHECK(cudaMemcpyAsync(b->sweep_cells, b->h_sweep, sizeof(SweepCell) * b->n_cells, cudaMemcpyHostToDevice,
+                            b->stream));
+   return sweep_device(b, b->sweep_cells, dim, per_cell, false);
+}
+
+int moments_device(vlgpu_batch* b, bool second) {
+   b->launches += 1;
+   VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, b->moments, b->mdev, b->vmin_d,
+                           b->bs_d, b->dv_d, b->params.mass, b->params.charge, second, b->n_cells, b->stream));
+   return VLGPU_OK;
+}
+
+int adjust_device(vlgpu_batch* b) {
+   const int a = b->adj_next;
+   b->adj_next = 1 - a;
+   VL_CHECK(cudaMemsetAsync(b->counters, 0, sizeof(SweepCounters), b->stream));
+   const double dv3 = b->dv_d[0] * b->dv_d[1] * b->dv_d[2];
+   VL_CHECK(launch_adjust(b->st_gids, b->st_src, b->st_slots, b->content_valid ? b->content : nullptr,
+                          b->data[b->cur], b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss, b->status,
+                          b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
+                          (int)b->params.add_width_v, dv3, b->n_cells, b->stream));
+   b->launches += 1;
+   b->st_gids = b->adj_gids[a];
+   b->st_src = b->adj_src[a];
+   b->st_slots = b->adj_slots[a];
+   b->content_valid = false;
+   return VLGPU_OK;
+}
+
+// Copies an indirect state's values into the other pool in list order.
+int materialize(vlgpu_batch* b) {
+   if (!b->st_src) return VLGPU_OK;
+   std::vector<CellSlot> slots(b->n_cells);
+   VL_CHECK(cudaMemcpyAsync(slots.data(), b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   uint64_t hi = 0;
+   for (const CellSlot& s : slots) hi = std::max<uint64_t>(hi, (uint64_t)s.off + s.count);
+   const int dst = 1 - b->cur;
+   VL_CHECK(launch_materialize(b->st_src, b->data[b->cur], b->data[dst], hi, b->stream));
+   b->launches += 1;
+   b->st_src = nullptr;
+   b->cur = dst;
+   return VLGPU_OK;
+}
+
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
+   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420)
+   int st = moments_device(b, false);
+   if (st != VLGPU_OK) return st;
+   b->launches += 1;
+   VL_CHECK(launch_geometry(b->accel_in, b->moments, b->isect12, b->sweep3, b->n_cells, b->params.charge,
+                            b->params.mass, b->params.hall_minimum_rhoq, (int)b->params.ohm_gradpe, MU_0, b->vmin_d,
+                            b->dv_d, map_order, (float)b->params.min_value, b->stream));
+   static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+   for (int s = 0; s < 3; ++s) {
+      const uint32_t d = orders[map_order][s];
+      st = sweep_device(b, b->sweep3 + (size_t)d * b->n_cells, d, per_cell, s == 0);
+      if (st != VLGPU_OK) return st;
+   }
+   // final block adjustment and moments (vlasovmover.cpp:564-569)
+   st = adjust_device(b);
+   if (st != VLGPU_OK) return st;
+   return moments_device(b, true);
+}
+
+int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      CellAccelInputs& a = b->h_accel[c];
+      for (int r = 0; r < 3; ++r) {
+         a.B[r] = fields[c].B[r];
+         a.curl[r] = fields[c].curl[r];
+         a.egradpe[r] = fields[c].egradpe[r];
+      }
+      a.dt = dt[c];
+   }
+   VL_CHECK(cudaMemcpyAsync(b->accel_in, b->h_accel, sizeof(CellAccelInputs) * b->n_cells, cudaMemcpyHostToDevice,
+                            b->stream));
+   return VLGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vlgpu_version(void) { return "vlgpu 0.2 (sm_100a)"; }
+
+int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint32_t n_cells, uint64_t block_capacity,
+                       int device, vlgpu_batch** out) {
+   if (!mesh || !params || !out || n_cells == 0 || block_capacity == 0 || block_capacity >= 0xffffffffull)
+      return VLGPU_EINVAL;
+   for (int d = 0; d < 3; ++d)
+      if (mesh->len[d] == 0 || mesh->len[d] > (uint32_t)MAX_LEN || !(mesh->vmax[d] > mesh->vmin[d]))
+         return VLGPU_EINVAL;
+   if (params->add_width_v > 31 || !(params->min_value > 0.0) || !(params->mass > 0.0)) return VLGPU_EINVAL;
+   int ndev = 0;
+   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return VLGPU_ENODEV;
+   if (device < 0 || device >= ndev) return VLGPU_EINVAL;
+   vlgpu_batch* b = new vlgpu_batch();
+   b->device = device;
+   b->mesh = *mesh;
+   b->params = *params;
+   b->n_cells = n_cells;
+   b->capacity = block_capacity;
+   for (int d = 0; d < 3; ++d) {
+      b->mdev.len[d] = mesh->len[d];
+      b->vmin_d[d] = mesh->vmin[d];
+      b->bs_d[d] = (mesh->vmax[d] - mesh->vmin[d]) / mesh->len[d];
+      b->dv_d[d] = b->bs_d[d] / WID;
+      b->mdev.dv[d] = (float)b->dv_d[d];
+      b->mdev.vmin[d] = (float)mesh->vmin[d];
+   }
+   auto fail = [&](cudaError_t e, const char* what) {
+      int s = cuda_status(e, what);
+      free_batch(b);
+      return s;
+   };
+   cudaError_t e = cudaSetDevice(device);
+   if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+   cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+   b->remap_grid = b->sm_count * remap_blocks_per_sm();
+   const uint64_t cap = block_capacity;
+   for (int p = 0; p < 2; ++p) {
+      if ((e = cudaMalloc(&b->gids[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "gids");
+      if ((e = cudaMalloc(&b->data[p], sizeof(float) * WID3 * cap)) != cudaSuccess) return fail(e, "data");
+      if ((e = cudaMalloc(&b->slots[p], sizeof(CellSlot) * n_cells)) != cudaSuccess) return fail(e, "slots");
+      if ((e = cudaMemset(b->slots[p], 0, sizeof(CellSlot) * n_cells)) != cudaSuccess) return fail(e, "slots");
+      if ((e = cudaMalloc(&b->adj_gids[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "adj");
+      if ((e = cudaMalloc(&b->adj_src[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "adj");
+      if ((e = cudaMalloc(&b->adj_slots[p], sizeof(CellSlot) * n_cells)) != cudaSuccess) return fail(e, "adj");
+   }
+   if ((e = cudaMalloc(&b->content, cap)) != cudaSuccess) return fail(e, "content");
+   if ((e = cudaMalloc(&b->perm, sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "perm");
+   if ((e = cudaMalloc(&b->sets, sizeof(ColumnSet) * cap)) != cudaSuccess) return fail(e, "sets");
+   if ((e = cudaMalloc(&b->sweep_cells, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "sweep");
+   if ((e = cudaMalloc(&b->sweep3, sizeof(SweepCell) * 3 * n_cells)) != cudaSuccess) return fail(e, "sweep3");
+   if ((e = cudaMalloc(&b->accel_in, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "accel");
+   if ((e = cudaMemset(b->accel_in, 0, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "accel");
+   if ((e = cudaMalloc(&b->moments, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMemset(b->moments, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMalloc(&b->isect12, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
+   if ((e = cudaMemset(b->isect12, 0, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
+   if ((e = cudaMalloc(&b->loss, sizeof(double) * n_cells)) != cudaSuccess) return fail(e, "loss");
+   if ((e = cudaMemset(b->loss, 0, sizeof(double) * n_cells)) != cudaSuccess) return fail(e, "loss");
+   if ((e = cudaMalloc(&b->status, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "status");
+   if ((e = cudaMemset(b->status, 0, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "status");
+   if ((e = cudaMalloc(&b->counters, sizeof(SweepCounters))) != cudaSuccess) return fail(e, "counters");
+   if ((e = cudaMalloc(&b->stats, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
+   if ((e = cudaMemset(b->stats, 0, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
+   if ((e = cudaMallocHost(&b->h_sweep, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "pinned");
+   if ((e = cudaMallocHost(&b->h_accel, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "pinned");
+   set_direct_state(b, 0);
+   *out = b;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_destroy(vlgpu_batch* b) {
+   if (!b) return VLGPU_EINVAL;
+   if (b->stream) cudaStreamSynchronize(b->stream);
+   free_batch(b);
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* gids, const float* data) {
+   if (!b || !offsets) return VLGPU_EINVAL;
+   const uint64_t total = offsets[b->n_cells];
+   if (total > b->capacity) return VLGPU_ENOMEM;
+   if (total > 0 && (!gids || !data)) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   std::vector<CellSlot> slots(b->n_cells);
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      if (offsets[c + 1] < offsets[c]) return VLGPU_EINVAL;
+      slots[c].off = (uint32_t)offsets[c];
+      slots[c].count = (uint32_t)(offsets[c + 1] - offsets[c]);
+   }
+   const uint32_t maxgid = b->mesh.len[0] * b->mesh.len[1] * b->mesh.len[2];
+   for (uint64_t q = 0; q < total; ++q)
+      if (gids[q] >= maxgid) return VLGPU_EINVAL;
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   VL_CHECK(cudaMemcpyAsync(b->gids[0], gids, sizeof(uint32_t) * total, cudaMemcpyHostToDevice, b->stream));
+   VL_CHECK(cudaMemcpyAsync(b->data[0], data, sizeof(float) * WID3 * total, cudaMemcpyHostToDevice, b->stream));
+   VL_CHECK(cudaMemcpyAsync(b->slots[0], slots.data(), sizeof(CellSlot) * b->n_cells, cudaMemcpyHostToDevice,
+                            b->stream));
+   VL_CHECK(cudaMemsetAsync(b->status, 0, sizeof(uint32_t) * b->n_cells, b->stream));
+   VL_CHECK(cudaMemsetAsync(b->loss, 0, sizeof(double) * b->n_cells, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   set_direct_state(b, 0);
+   b->content_valid = false;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_block_counts(vlgpu_batch* b, uint32_t* counts) {
+   if (!b || !counts) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   std::vector<CellSlot> slots(b->n_cells);
+   VL_CHECK(cudaMemcpyAsync(slots.data(), b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   for (uint32_t c = 0; c < b->n_cells; ++c) counts[c] = slots[c].count;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_status(vlgpu_batch* b, uint32_t* status) {
+   if (!b || !status) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaMemcpyAsync(status, b->status, sizeof(uint32_t) * b->n_cells, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_download_raw(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
+                             uint64_t capacity, uint64_t* used) {
+   if (!b || !cell_off || !cell_count || !used) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   int st = materialize(b);
+   if (st != VLGPU_OK) return st;
+   std::vector<CellSlot> slots(b->n_cells);
+   VL_CHECK(cudaMemcpyAsync(slots.data(), b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   uint64_t hi = 0;
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      cell_off[c] = slots[c].off;
+      cell_count[c] = slots[c].count;
+      hi = std::max<uint64_t>(hi, (uint64_t)slots[c].off + slots[c].count);
+   }
+   *used = hi;
+   if (hi > capacity) return VLGPU_ENOMEM;
+   if (hi > 0 && (!gids || !data)) return VLGPU_EINVAL;
+   VL_CHECK(cudaMemcpyAsync(gids, b->st_gids, sizeof(uint32_t) * hi, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaMemcpyAsync(data, b->data[b->cur], sizeof(float) * WID3 * hi, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_download(vlgpu_batch* b, uint64_t* offsets, uint32_t* gids, float* data, uint64_t capacity) {
+   if (!b || !offsets) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   int st = materialize(b);
+   if (st != VLGPU_OK) return st;
+   std::vector<CellSlot> slots(b->n_cells);
+   VL_CHECK(cudaMemcpyAsync(slots.data(), b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   uint64_t total = 0, hi = 0;
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      total += slots[c].count;
+      hi = std::max<uint64_t>(hi, (uint64_t)slots[c].off + slots[c].count);
+   }
+   offsets[0] = 0;
+   for (uint32_t c = 0; c < b->n_cells; ++c) offsets[c + 1] = offsets[c] + slots[c].count;
+   if (total > capacity) return VLGPU_ENOMEM;
+   if (total > 0 && (!gids || !data)) return VLGPU_EINVAL;
+   std::vector<uint32_t> g(hi);
+   std::vector<float> d((size_t)hi * WID3);
+   VL_CHECK(cudaMemcpyAsync(g.data(), b->st_gids, sizeof(uint32_t) * hi, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaMemcpyAsync(d.data(), b->data[b->cur], sizeof(float) * WID3 * hi, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   std::vector<uint32_t> order;
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      const CellSlot s = slots[c];
+      order.resize(s.count);
+      std::iota(order.begin(), order.end(), 0u);
+      std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return g[s.off + x] < g[s.off + y]; });
+      for (uint32_t q = 0; q < s.count; ++q) {
+         gids[offsets[c] + q] = g[s.off + order[q]];
+         std::memcpy(data + (offsets[c] + q) * WID3, d.data() + (size_t)(s.off + order[q]) * WID3,
+                     sizeof(float) * WID3);
+      }
+   }
+   return VLGPU_OK;
+}
+
+int vlgpu_map_1d(vlgpu_batch* b, const double* intersections, uint32_t dimension) {
+   if (!b || !intersections || dimension > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return run_sweep(b, intersections, 4, dimension, false);
+}
+
+int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t dimension) {
+   if (!b || !intersections || dimension > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return run_sweep(b, intersections, 4, dimension, true);
+}
+
+int vlgpu_accelerate_with_intersections(vlgpu_batch* b, const double* intersections12, uint32_t map_order) {
+   if (!b || !intersections12 || map_order > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+   for (int s = 0; s < 3; ++s) {
+      const uint32_t d = orders[map_order][s];
+      int st = run_sweep(b, intersections12 + 4 * d, 12, d, false);
+      if (st != VLGPU_OK) return st;
+   }
+   return VLGPU_OK;
+}
+
+int vlgpu_accelerate(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt, uint32_t map_order) {
+   if (!b || !fields || !dt || map_order > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   int st = stage_fields(b, fields, dt);
+   if (st != VLGPU_OK) return st;
+   return accelerate_device(b, map_order, false);
+}
+
+int vlgpu_accelerate_device(vlgpu_batch* b, uint32_t map_order) {
+   if (!b || map_order > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return accelerate_device(b, map_order, false);
+}
+
+int vlgpu_accelerate_per_cell(vlgpu_batch* b, uint32_t map_order) {
+   if (!b || map_order > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return accelerate_device(b, map_order, true);
+}
+
+int vlgpu_adjust_blocks(vlgpu_batch* b) {
+   if (!b) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return adjust_device(b);
+}
+
+int vlgpu_batch_rho_loss(vlgpu_batch* b, double* out) {
+   if (!b || !out) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaMemcpyAsync(out, b->loss, sizeof(double) * b->n_cells, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16) {
+   if (!b || !out16) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   int st = moments_device(b, compute_second != 0);
+   if (st != VLGPU_OK) return st;
+   VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_intersections(vlgpu_batch* b, double* out12) {
+   if (!b || !out12) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaMemcpyAsync(out12, b->isect12, sizeof(double) * 12 * b->n_cells, cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_stream(vlgpu_batch* b, void** stream) {
+   if (!b || !stream) return VLGPU_EINVAL;
+   *stream = (void*)b->stream;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_profile(vlgpu_batch* b, int enable) {
+   if (!b) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   if (enable && b->prof_events.empty()) {
+      b->prof_events.resize(4096);
+      for (auto& ev : b->prof_events) VL_CHECK(cudaEventCreate(&ev));
+   }
+   b->profiling = enable != 0;
+   b->prof_used = 0;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_stats(vlgpu_batch* b, uint64_t* out8) {
+   if (!b || !out8) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   BatchStats st{};
+   VL_CHECK(cudaMemcpy(&st, b->stats, sizeof(st), cudaMemcpyDeviceToHost));
+   double ms = 0.0;
+   for (size_t q = 0; q + 1 < b->prof_used; q += 2) {
+      float t = 0.f;
+      VL_CHECK(cudaEventElapsedTime(&t, b->prof_events[q], b->prof_events[q + 1]));
+      ms += t;
+   }
+   out8[0] = b->launches;
+   out8[1] = st.sweeps;
+   out8[2] = st.src_blocks;
+   out8[3] = st.dst_blocks;
+   out8[4] = b->remap_launches;
+   out8[5] = (uint64_t)(ms * 1e6);
+   out8[6] = b->prof_used / 2;
+   out8[7] = st.sets;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out) {
+   if (!b || !out) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   BatchStats st{};
+   VL_CHECK(cudaMemcpy(&st, b->stats, sizeof(st), cudaMemcpyDeviceToHost));
+   out[0] = st.step_blocks;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_sync(vlgpu_batch* b) {
+   if (!b) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   SweepCounters c{};
+   VL_CHECK(cudaMemcpy(&c, b->counters, sizeof(c), cudaMemcpyDeviceToHost));
+   if (c.overflow) return VLGPU_ENOMEM;
+   return VLGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// Shared device-side definitions for the vlgpu kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/vlgpu.h"
+
+namespace vlgpu {
+
+constexpr int WID = 4;
+constexpr int WID2 = 16;
+constexpr int WID3 = 64;
+constexpr int MAX_LEN = 96;         // blocks per mesh axis supported by the 3-word column masks
+constexpr int MAX_PLANE = 96 * 96;  // transverse plane entries
+
+// Per-cell state of one batch, indexed by cell.
+struct CellSlot {
+   uint32_t off;     // first block in the current pool
+   uint32_t count;   // number of blocks
+};
+
+// One column set of one sweep: all blocks of a cell that share the two
+// transverse block indices.  Built by the columnize kernel, consumed by the
+// remap kernel.
+struct ColumnSet {
+   uint32_t cell;
+   uint32_t si, sj;     // transverse block indices in the swapped frame
+   uint32_t src_pos;    // first entry in the permutation array (absolute)
+   uint32_t dst_pos;    // first output block (absolute, destination pool)
+   uint32_t src_mask[3];
+   uint32_t tgt_mask[3];
+};
+
+// Per-cell sweep parameters, already converted to Realf and swapped into the
+// frame where the sweep dimension is k (cpu_acc_map.cpp:127-199).
+struct SweepCell {
+   float intersection, di, dj, dk;
+   float threshold;
+   uint32_t pad;
+};
+
+// Mesh constants used on the device (cell size and origin already in Realf).
+struct MeshDev {
+   uint32_t len[3];
+   float dv[3];
+   float vmin[3];
+};
+
+// Counters of one sweep, zeroed before the columnize launch.
+struct SweepCounters {
+   uint32_t n_sets;
+   uint32_t dst_top;
+   uint32_t work;
+   uint32_t overflow;
+};
+
+// Running totals kept on the device across sweeps (never reset by a sweep).
+struct BatchStats {
+   unsigned long long src_blocks;  // source blocks entering sweeps
+   unsigned long long dst_blocks;  // blocks written by sweeps
+   unsigned long long sweeps;      // cell-sweeps performed
+   unsigned long long sets;        // column sets remapped
+   unsigned long long step_blocks; // blocks entering the first sweep of each acceleration step
+};
+
+__host__ __device__ inline void swapped_indices(uint32_t gid, const uint32_t len[3], int dim, uint32_t s[3]) {
+   const uint32_t x = gid % len[0];
+   const uint32_t y = (gid / len[0]) % len[1];
+   const uint32_t z = gid / (len[0] * len[1]);
+   if (dim == 0) { s[0] = z; s[1] = y; s[2] = x; }
+   else if (dim == 1) { s[0] = x; s[1] = z; s[2] = y; }
+   else { s[0] = x; s[1] = y; s[2] = z; }
+}
+
+__host__ __device__ inline uint32_t gid_from_swapped(uint32_t a, uint32_t b, uint32_t k, const uint32_t len[3], int dim) {
+   uint32_t x, y, z;
+   if (dim == 0) { z = a; y = b; x = k; }
+   else if (dim == 1) { x = a; z = b; y = k; }
+   else { x = a; y = b; z = k; }
+   return x + len[0] * (y + len[1] * z);
+}
+
+// Transverse lengths (i, j) of the swapped frame.
+__host__ __device__ inline void plane_lengths(const uint32_t len[3], int dim, uint32_t& li, uint32_t& lj) {
+   if (dim == 0) { li = len[2]; lj = len[1]; }
+   else if (dim == 1) { li = len[0]; lj = len[2]; }
+   else { li = len[0]; lj = len[1]; }
+}
+
+__device__ inline int mask_popc_below(const uint32_t m[3], uint32_t k) {
+   int n = 0;
+   const uint32_t w = k >> 5, b = k & 31;
+   if (w > 0) n += __popc(m[0]);
+   if (w > 1) n += __popc(m[1]);
+   n += __popc(m[w] & ((1u << b) - 1u));
+   return n;
+}
+
+}  // namespace vlgpu

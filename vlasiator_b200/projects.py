@@ -102,10 +102,14 @@ def maxwellian_cell(mesh: VelocityMesh, n: float, T: float, V, min_value: float 
     occ[ck, cj, ci] = True
     keep = _dilate(occ, add_width)
     kz, ky, kx = np.nonzero(keep)
-    gids = np.sort(mesh.gid(kx, ky, kz).astype(np.uint32))
-    vx, vy, vz = mesh.cell_centres(gids.astype(np.int64))
-    data = maxwellian_density(vx, vy, vz, n, T, V, mass, T_aniso).astype(dtype)
-    return CellState(gids=gids, data=np.ascontiguousarray(data.reshape(-1, WID3)), V=V.copy(), n=n, T=T)
+    gids = np.sort(mesh.gid(kx, ky, kz).astype(np.int64))
+    # the candidate box already spans one block beyond every content block,
+    # so every kept block was evaluated above (cand is sorted by GID)
+    order = np.argsort(cand)
+    pos = order[np.searchsorted(cand[order], gids)]
+    data = f[pos]
+    return CellState(gids=gids.astype(np.uint32), data=np.ascontiguousarray(data.reshape(-1, WID3)), V=V.copy(),
+                     n=n, T=T)
 
 
 def larmor_cell(mesh: VelocityMesh | None = None) -> CellState:

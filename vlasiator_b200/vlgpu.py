@@ -1,0 +1,277 @@
+"""Host-side binding of libvlgpu.so (the CUDA hot path) through its C ABI.
+
+``Batch`` mirrors what the reference's solver drivers act on: a set of
+spatial cells, each with one population's velocity mesh (block global IDs)
+and block container (64 Realf per block).  Its methods map one to one onto
+the reference's entry points for that data:
+
+* ``map_1d(intersections, dim)``    -> map_1d per cell (vlasovsolver/cpu_acc_map.cpp:121)
+* ``accelerate_with_intersections`` -> cpu_accelerate_cell (vlasovsolver/cpu_acc_semilag.cpp:92)
+
+The library must be built for sm_100a (``python -m vlasiator_b200.build``);
+there is no CPU fallback, and every call raises on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .mesh import WID3, VelocityMesh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvlgpu.so")
+
+STATUS = {0: "VLGPU_OK", 1: "VLGPU_EINVAL", 2: "VLGPU_ENOMEM", 3: "VLGPU_EWALL", 4: "VLGPU_ETIMEDOUT",
+          5: "VLGPU_ERANGE", 6: "VLGPU_ECUDA", 7: "VLGPU_ENODEV"}
+CELL_WALL, CELL_RANGE, CELL_NOMEM, CELL_BADDK = 1, 2, 4, 8
+
+
+class VlgpuError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {STATUS.get(code, code)}")
+        self.code = code
+
+
+class CMeshT(ctypes.Structure):
+    _fields_ = [("vmin", ctypes.c_double * 3), ("vmax", ctypes.c_double * 3), ("len", ctypes.c_uint32 * 3)]
+
+
+class CParamsT(ctypes.Structure):
+    _fields_ = [("charge", ctypes.c_double), ("mass", ctypes.c_double), ("min_value", ctypes.c_double),
+                ("add_width_v", ctypes.c_uint32), ("wall_margin", ctypes.c_uint32),
+                ("hall_minimum_rhoq", ctypes.c_double), ("ohm_gradpe", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class CFieldsT(ctypes.Structure):
+    _fields_ = [("B", ctypes.c_double * 3), ("curl", ctypes.c_double * 3), ("egradpe", ctypes.c_double * 3)]
+
+
+_lib = None
+
+# every symbol include/vlgpu.h declares, with its ctypes signature
+_vp = ctypes.c_void_p
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "vlgpu_batch_create": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32,
+                                          ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "vlgpu_batch_destroy": (ctypes.c_int, [_vp]),
+    "vlgpu_batch_upload": (ctypes.c_int, [_vp, _u64p, _u32p, _fp]),
+    "vlgpu_batch_block_counts": (ctypes.c_int, [_vp, _u32p]),
+    "vlgpu_batch_download": (ctypes.c_int, [_vp, _u64p, _u32p, _fp, ctypes.c_uint64]),
+    "vlgpu_batch_status": (ctypes.c_int, [_vp, _u32p]),
+    "vlgpu_map_1d": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
+    "vlgpu_map_1d_per_cell": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
+    "vlgpu_accelerate_with_intersections": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
+    "vlgpu_accelerate": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), _dp, ctypes.c_uint32]),
+    "vlgpu_accelerate_device": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "vlgpu_accelerate_per_cell": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "vlgpu_adjust_blocks": (ctypes.c_int, [_vp]),
+    "vlgpu_batch_rho_loss": (ctypes.c_int, [_vp, _dp]),
+    "vlgpu_batch_moments": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "vlgpu_batch_intersections": (ctypes.c_int, [_vp, _dp]),
+    "vlgpu_batch_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "vlgpu_batch_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "vlgpu_batch_stats": (ctypes.c_int, [_vp, _u64p]),
+    "vlgpu_batch_stats2": (ctypes.c_int, [_vp, _u64p]),
+    "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
+    "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
+    "vlgpu_version": (ctypes.c_char_p, []),
+}
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libvlgpu.so; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: build it with `python -m vlasiator_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code: int, what: str):
+    if code != 0:
+        raise VlgpuError(code, what)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def make_params(charge=1.60217653e-19, mass=1.67262158e-27, min_value=1e-15, add_width_v=1, wall_margin=1,
+                hall_minimum_rhoq=1.60217653e-19, ohm_gradpe=0) -> CParamsT:
+    p = CParamsT()
+    p.charge, p.mass, p.min_value = charge, mass, min_value
+    p.add_width_v, p.wall_margin = add_width_v, wall_margin
+    p.hall_minimum_rhoq, p.ohm_gradpe = hall_minimum_rhoq, ohm_gradpe
+    return p
+
+
+class Batch:
+    """A device-resident batch of spatial cells (one population)."""
+
+    def __init__(self, mesh: VelocityMesh, n_cells: int, capacity: int, params: CParamsT | None = None,
+                 device: int = 0):
+        self.lib = load()
+        self.mesh = mesh
+        self.n_cells = int(n_cells)
+        self.capacity = int(capacity)
+        m = CMeshT()
+        for d in range(3):
+            m.vmin[d], m.vmax[d], m.len[d] = mesh.vmin[d], mesh.vmax[d], mesh.length[d]
+        self.params = params or make_params()
+        h = _vp()
+        _check(self.lib.vlgpu_batch_create(ctypes.byref(m), ctypes.byref(self.params), self.n_cells, self.capacity,
+                                           device, ctypes.byref(h)), "vlgpu_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.vlgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- data movement ----
+    def upload(self, gid_list, data_list):
+        offs = np.zeros(self.n_cells + 1, np.uint64)
+        offs[1:] = np.cumsum([len(g) for g in gid_list])
+        gids = np.ascontiguousarray(np.concatenate(gid_list).astype(np.uint32))
+        data = np.ascontiguousarray(np.concatenate([np.asarray(d, np.float32).reshape(-1, WID3) for d in data_list]))
+        _check(self.lib.vlgpu_batch_upload(self.h, _p(offs, ctypes.c_uint64), _p(gids, ctypes.c_uint32),
+                                           _p(data, ctypes.c_float)), "vlgpu_batch_upload")
+
+    def upload_packed(self, offsets, gids, data):
+        offs = np.ascontiguousarray(offsets, np.uint64)
+        gids = np.ascontiguousarray(gids, np.uint32)
+        data = np.ascontiguousarray(data, np.float32)
+        _check(self.lib.vlgpu_batch_upload(self.h, _p(offs, ctypes.c_uint64), _p(gids, ctypes.c_uint32),
+                                           _p(data, ctypes.c_float)), "vlgpu_batch_upload")
+
+    def block_counts(self) -> np.ndarray:
+        c = np.zeros(self.n_cells, np.uint32)
+        _check(self.lib.vlgpu_batch_block_counts(self.h, _p(c, ctypes.c_uint32)), "vlgpu_batch_block_counts")
+        return c
+
+    def status(self) -> np.ndarray:
+        s = np.zeros(self.n_cells, np.uint32)
+        _check(self.lib.vlgpu_batch_status(self.h, _p(s, ctypes.c_uint32)), "vlgpu_batch_status")
+        return s
+
+    def download(self):
+        """Returns (offsets, gids, data) with blocks sorted by GID inside each cell."""
+        total = int(self.block_counts().astype(np.uint64).sum())
+        offs = np.zeros(self.n_cells + 1, np.uint64)
+        gids = np.zeros(max(total, 1), np.uint32)
+        data = np.zeros((max(total, 1), WID3), np.float32)
+        _check(self.lib.vlgpu_batch_download(self.h, _p(offs, ctypes.c_uint64), _p(gids, ctypes.c_uint32),
+                                             _p(data, ctypes.c_float), max(total, 1)), "vlgpu_batch_download")
+        return offs, gids[:total], data[:total]
+
+    def download_raw(self, gids_out=None, data_out=None):
+        """Unsorted copy of the current pool: (cell_off, cell_count, gids, data) views."""
+        off = np.zeros(self.n_cells, np.uint32)
+        cnt = np.zeros(self.n_cells, np.uint32)
+        used = ctypes.c_uint64(0)
+        if gids_out is None:
+            gids_out = np.zeros(self.capacity, np.uint32)
+            data_out = np.zeros((self.capacity, WID3), np.float32)
+        _check(self.lib.vlgpu_batch_download_raw(self.h, _p(off, ctypes.c_uint32), _p(cnt, ctypes.c_uint32),
+                                                 _p(gids_out, ctypes.c_uint32), _p(data_out, ctypes.c_float),
+                                                 len(gids_out), ctypes.byref(used)), "vlgpu_batch_download_raw")
+        u = int(used.value)
+        return off, cnt, gids_out[:u], data_out[:u]
+
+    def cells(self):
+        offs, g, d = self.download()
+        return [(g[offs[c]:offs[c + 1]], d[offs[c]:offs[c + 1]]) for c in range(self.n_cells)]
+
+    # ---- the hot path ----
+    def map_1d(self, intersections, dim: int, per_cell: bool = False):
+        I = np.ascontiguousarray(intersections, np.float64).reshape(self.n_cells, 4)
+        fn = self.lib.vlgpu_map_1d_per_cell if per_cell else self.lib.vlgpu_map_1d
+        _check(fn(self.h, _p(I, ctypes.c_double), dim), "vlgpu_map_1d")
+
+    def accelerate_with_intersections(self, intersections12, map_order: int):
+        I = np.ascontiguousarray(intersections12, np.float64).reshape(self.n_cells, 12)
+        _check(self.lib.vlgpu_accelerate_with_intersections(self.h, _p(I, ctypes.c_double), map_order),
+               "vlgpu_accelerate_with_intersections")
+
+    def accelerate(self, B, dt, map_order: int, curl=None, egradpe=None):
+        """One acceleration step (moments -> FP64 geometry -> three sweeps) of every cell."""
+        n = self.n_cells
+        F = (CFieldsT * n)()
+        B = np.asarray(B, np.float64).reshape(n, 3)
+        curl = np.zeros((n, 3)) if curl is None else np.asarray(curl, np.float64).reshape(n, 3)
+        eg = np.zeros((n, 3)) if egradpe is None else np.asarray(egradpe, np.float64).reshape(n, 3)
+        for c in range(n):
+            for r in range(3):
+                F[c].B[r], F[c].curl[r], F[c].egradpe[r] = B[c, r], curl[c, r], eg[c, r]
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (n,)))
+        _check(self.lib.vlgpu_accelerate(self.h, F, _p(dt, ctypes.c_double), map_order), "vlgpu_accelerate")
+
+    def accelerate_device(self, map_order: int, per_cell: bool = False):
+        fn = self.lib.vlgpu_accelerate_per_cell if per_cell else self.lib.vlgpu_accelerate_device
+        _check(fn(self.h, map_order), "vlgpu_accelerate_device")
+
+    def adjust(self):
+        _check(self.lib.vlgpu_adjust_blocks(self.h), "vlgpu_adjust_blocks")
+
+    def rho_loss(self) -> np.ndarray:
+        out = np.zeros(self.n_cells)
+        _check(self.lib.vlgpu_batch_rho_loss(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_rho_loss")
+        return out
+
+    def moments(self, second: bool = True) -> np.ndarray:
+        out = np.zeros((self.n_cells, 16))
+        _check(self.lib.vlgpu_batch_moments(self.h, int(second), _p(out, ctypes.c_double)), "vlgpu_batch_moments")
+        return out
+
+    def intersections(self) -> np.ndarray:
+        out = np.zeros((self.n_cells, 12))
+        _check(self.lib.vlgpu_batch_intersections(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_intersections")
+        return out
+
+    def stream_handle(self) -> int:
+        s = _vp()
+        _check(self.lib.vlgpu_batch_stream(self.h, ctypes.byref(s)), "vlgpu_batch_stream")
+        return int(s.value or 0)
+
+    def profile(self, enable: bool = True):
+        _check(self.lib.vlgpu_batch_profile(self.h, int(enable)), "vlgpu_batch_profile")
+
+    def stats(self) -> dict:
+        o = np.zeros(8, np.uint64)
+        _check(self.lib.vlgpu_batch_stats(self.h, _p(o, ctypes.c_uint64)), "vlgpu_batch_stats")
+        keys = ["launches", "cell_sweeps", "src_blocks", "dst_blocks", "remap_launches", "remap_ns",
+                "remap_profiled", "sets"]
+        d = {k: int(v) for k, v in zip(keys, o)}
+        o2 = np.zeros(1, np.uint64)
+        _check(self.lib.vlgpu_batch_stats2(self.h, _p(o2, ctypes.c_uint64)), "vlgpu_batch_stats2")
+        d["step_blocks"] = int(o2[0])
+        return d
+
+    def sync(self):
+        _check(self.lib.vlgpu_batch_sync(self.h), "vlgpu_batch_sync")
