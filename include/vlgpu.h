@@ -126,6 +126,13 @@ int vlgpu_accelerate_with_intersections(vlgpu_batch* b, const double* intersecti
    per cell (Population::subcycleDt); host memory. */
 int vlgpu_accelerate(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt, uint32_t map_order);
 
+/* Only the geometry part of that step: pivot moments, FP64 transform and the
+   three intersection sets of every cell (compute_cell_intersections,
+   vlasovsolver/cpu_acc_intersections.cpp:44-101), readable with
+   vlgpu_batch_intersections; the VDF is not changed. */
+int vlgpu_compute_intersections(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt,
+                                uint32_t map_order);
+
 /* The same step reusing the fields and dt last passed to vlgpu_accelerate
    (no host data; suitable for stream capture). */
 int vlgpu_accelerate_device(vlgpu_batch* b, uint32_t map_order);

@@ -24,7 +24,7 @@ mkdir -p "$SRC/vlasovsolver" "$SRC/spatial_cells" "$SRC/arch" "$SRC/sysinc"
 for f in cpu_acc_map.cpp cpu_acc_map.hpp cpu_acc_sort_blocks.cpp cpu_acc_sort_blocks.hpp \
          cpu_acc_load_blocks.cpp cpu_acc_load_blocks.hpp cpu_1d_plm.hpp cpu_1d_ppm.hpp \
          cpu_1d_pqm.hpp cpu_1d_ppm_nonuniform.hpp cpu_face_estimates.hpp cpu_slope_limiters.hpp \
-         vec.h vectorclass_fallback.h arch_moments.h; do
+         vec.h vectorclass_fallback.h arch_moments.h cpu_trans_map_amr.hpp cpu_trans_pencils.hpp; do
   ln -s "$REF/vlasovsolver/$f" "$SRC/vlasovsolver/$f"
 done
 for f in velocity_mesh_cpu.h velocity_block_container.h; do
@@ -36,6 +36,11 @@ done
 for f in arch_device_api.h arch_device_host.h; do
   ln -s "$REF/arch/$f" "$SRC/arch/$f"
 done
+# translation: the uniform-grid part of cpu_trans_map_amr.cpp (propagatePencil,
+# copy_trans_block_data_amr, trans_map_1d_amr; lines 1-443), without the MPI
+# remote-contribution functions that follow
+sed -n '1,443p' "$REF/vlasovsolver/cpu_trans_map_amr.cpp" > "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp"
+cp "$HERE/ref_shim/grid.h" "$SRC/grid.h"
 cp "$HERE/ref_shim/object_wrapper.h" "$SRC/object_wrapper.h"
 cp "$HERE/ref_shim/spatial_cells/spatial_cell_wrapper.hpp" "$SRC/spatial_cells/spatial_cell_wrapper.hpp"
 cp "$HERE/ref_shim/sysinc/"*.hpp "$SRC/sysinc/"
@@ -47,7 +52,7 @@ COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
         -I"$SRC" -I"$SRC/sysinc" -w)
 SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
       "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
-      "$SRC/velocity_mesh_parameters.cpp")
+      "$SRC/velocity_mesh_parameters.cpp" "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp")
 # the oracle's own FP64 geometry restatement (the reference's needs Eigen)
 CC="${REF_CC:-/usr/bin/gcc}"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_sp.o"

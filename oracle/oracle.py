@@ -60,6 +60,9 @@ class Restatement:
         L.orc_moments.restype = None
         L.orc_moments.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
                                   ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_translate.restype = ctypes.c_int
+        L.orc_translate.argtypes = [ctypes.POINTER(CMesh), _u32p, ctypes.POINTER(ctypes.c_uint64), _u32p,
+                                    ctypes.POINTER(ct), ctypes.c_uint32, ct, ct, ctypes.c_double, ctypes.POINTER(ct)]
         L.orc_adjust.restype = ctypes.c_int
         L.orc_adjust.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
                                  ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, ctypes.POINTER(ct), _dp]
@@ -106,6 +109,21 @@ class Restatement:
         if rc != 0:
             raise RuntimeError(f"orc_adjust failed with status {rc}")
         return go[: n.value].copy(), do[: n.value].copy(), loss.value
+
+    def translate(self, mesh: VelocityMesh, grid, offsets, gids, data, dim, dt, dz, min_value=1e-15):
+        """One spatial dimension of the translation of a uniform periodic grid (cells x fastest)."""
+        g3 = np.ascontiguousarray(grid, np.uint32)
+        offs = np.ascontiguousarray(offsets, np.uint64)
+        gids = np.ascontiguousarray(gids, np.uint32)
+        data = np.ascontiguousarray(data, self.realf).reshape(-1, WID3)
+        out = np.zeros_like(data)
+        cm = CMesh.of(mesh)
+        rc = self.lib.orc_translate(ctypes.byref(cm), _ptr(g3, ctypes.c_uint32), _ptr(offs, ctypes.c_uint64),
+                                    _ptr(gids, ctypes.c_uint32), _ptr(data, self._ct), dim, self._ct(dt),
+                                    self._ct(dz), float(min_value), _ptr(out, self._ct))
+        if rc != 0:
+            raise RuntimeError(f"orc_translate failed with status {rc}")
+        return out
 
     def accelerate_step(self, mesh: VelocityMesh, gids, data, B, dt, map_order, mass, charge, min_value=1e-15,
                         add_width=1, hall_min_rhoq=1.60217653e-19, mu0=1.25663706e-6):
@@ -179,6 +197,8 @@ class ReferenceBuild:
         L.ref_cells_accelerate_step.argtypes = [_vp, _dp, _dp, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_int]
         L.ref_max_threads.restype = ctypes.c_int
+        L.ref_cells_translate.argtypes = [_vp, _u32p, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int]
 
     def init(self, mesh: VelocityMesh, wall_margin: int = 1):
         vmin = np.array(mesh.vmin, np.float64)
@@ -223,6 +243,10 @@ class ReferenceBuild:
         dt = np.ascontiguousarray(dt, np.float64)
         self.lib.ref_cells_accelerate_step(h, _ptr(B, ctypes.c_double), _ptr(dt, ctypes.c_double), map_order,
                                            charge, mass, nthreads)
+
+    def translate(self, h, grid, dim, dt, dz, nthreads=0):
+        g = np.ascontiguousarray(grid, np.uint32)
+        self.lib.ref_cells_translate(h, _ptr(g, ctypes.c_uint32), dim, float(dt), float(dz), nthreads)
 
     def max_threads(self) -> int:
         return self.lib.ref_max_threads()

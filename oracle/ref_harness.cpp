@@ -18,6 +18,8 @@
 #include "object_wrapper.h"
 #include "vlasovsolver/cpu_acc_map.hpp"
 #include "vlasovsolver/arch_moments.h"
+#include "vlasovsolver/cpu_trans_map_amr.hpp"
+#include "vlasovsolver/cpu_trans_pencils.hpp"
 
 using spatial_cell::SpatialCell;
 
@@ -45,6 +47,7 @@ void bailout(const bool condition, const char* const f, const int l) { bailout(c
 void memory_purge() {}
 
 static bool g_mesh_ready = false;
+std::array<setOfPencils, 3> DimensionPencils;
 
 extern "C" {
 
@@ -216,5 +219,50 @@ void ref_cells_accelerate_step(void* h, const double* B, const double* dt, uint3
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+// Translation of a uniform periodic grid along one dimension with the
+// reference's own trans_map_1d_amr (vlasovsolver/cpu_trans_map_amr.cpp:214-443).
+// Cells are x fastest and hold the blocks of the cell set `h` (cell c has
+// dccrg id c+1).  One pencil per grid line, padded with the periodic
+// neighbours (two on each side, the outer ones pure sources), as the
+// reference's pencil builder produces for a periodic dimension.
+void ref_cells_translate(void* h, const uint32_t grid[3], uint32_t dimension, double dt, double dz, int nthreads) {
+   RefCells* rc = (RefCells*)h;
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+   dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry> g;
+   std::vector<CellID> local;
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      g.cells[c + 1] = rc->cells[c];
+      local.push_back(c + 1);
+   }
+   const uint32_t nx = grid[0], ny = grid[1], nz = grid[2];
+   const uint32_t N = grid[dimension];
+   const uint64_t stride = dimension == 0 ? 1 : (dimension == 1 ? nx : (uint64_t)nx * ny);
+   const uint32_t n_lines = (uint32_t)(rc->cells.size() / N);
+   setOfPencils& P = DimensionPencils[dimension];
+   P.removeAllPencils();
+   for (uint32_t p = 0; p < n_lines; ++p) {
+      uint64_t c0;
+      if (dimension == 0) c0 = (uint64_t)p * nx;
+      else if (dimension == 1) c0 = (uint64_t)(p % nx) + (uint64_t)nx * ny * (p / nx);
+      else c0 = p;
+      std::vector<CellID> ids;
+      for (uint32_t x = 0; x < N; ++x) ids.push_back(c0 + x * stride + 1);
+      P.addPencil(ids, 0.0, 0.0, false, std::vector<uint>());
+      const uint start = P.idsStart.back(), L = P.lengthOfPencils.back();
+      for (int s = 0; s < VLASOV_STENCIL_WIDTH; ++s) {
+         P.ids[start + s] = c0 + ((N - VLASOV_STENCIL_WIDTH + s) % N) * stride + 1;
+         P.ids[start + L - VLASOV_STENCIL_WIDTH + s] = c0 + ((uint64_t)s % N) * stride + 1;
+      }
+      for (uint q = 0; q < L; ++q) {
+         P.sourceDZ[start + q] = (Realf)dz;
+         P.targetRatios[start + q] = (q == 0 || q + 1 == L) ? 0.0 : 1.0;
+      }
+   }
+   P.binPencils();
+   std::vector<uint> nPencils(local.size() + 1, 0);
+   trans_map_1d_amr(g, local, std::vector<CellID>(), nPencils, dimension, (Realf)dt, 0);
+   (void)nz;
+}
 
 }  // extern "C"

@@ -9,6 +9,9 @@
 #pragma once
 #include <array>
 #include <vector>
+#include <dccrg.hpp>
+#include <dccrg_cartesian_geometry.hpp>
+#include <phiprof.hpp>
 #include "../common.h"
 #include "../memoryallocation.h"
 #include "velocity_mesh_cpu.h"
@@ -60,6 +63,9 @@ class SpatialCell {
       return populations[popID]->vmesh->getLocalID(gid);
    }
    Realf* get_data(const uint popID) { return populations[popID]->blockContainer->getData(); }
+   Realf* get_data(const vmesh::LocalID lid, const uint popID) {
+      return populations[popID]->blockContainer->getData(lid);
+   }
    bool add_velocity_block(const vmesh::GlobalID& gid, const uint popID) {
       Population& p = *populations[popID];
       if (!p.vmesh->push_back(gid)) return false;
@@ -84,3 +90,6 @@ class SpatialCell {
 };
 
 }  // namespace spatial_cell
+
+// the reference's own headers name the cell type unqualified
+using spatial_cell::SpatialCell;

@@ -735,3 +735,167 @@ int orc_adjust(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf*
    free(keep);
    return status;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Spatial translation on a uniform, periodic grid: one dimension of         */
+/* trans_map_1d_amr (vlasovsolver/cpu_trans_map_amr.cpp:214-443) with        */
+/* propagatePencil (:37-150) and compute_ppm_coeff_nonuniform                 */
+/* (cpu_1d_ppm_nonuniform.hpp:40-62, faces cpu_face_estimates.hpp:179-191,    */
+/* 327-378).  Every cell has width dz along the dimension and target ratio 1. */
+/* Cells are x fastest; cell c owns blocks offsets[c]..offsets[c+1]-1 (any    */
+/* order).  Block sets do not change; mass entering a cell that lacks the     */
+/* block is dropped, as in the reference.  data_out has the layout of data.   */
+/* ------------------------------------------------------------------------- */
+static realf h4_face_nonuniform(const realf* h, const realf* u) {
+   /* h[-2..1], u[-2..1]: left face of cell 0 (White et al. 2008 eq. 45) */
+   const double D1 = 1.0 / (h[-2] + h[-1] + h[0] + h[1]);
+   const realf F1 = (h[-2] + h[-1]) * (h[0] + h[1]) / (h[-1] + h[0]);
+   const realf V1 = F1 * (u[-1] * h[0] + u[0] * h[-1]);
+   const double D2 = 1.0 / (h[-2] + h[-1] + h[0]) + 1.0 / (h[-1] + h[0] + h[1]);
+   const realf V2 = (realf)((double)V1 * D2);
+   const realf F2 = (h[0] * (h[0] + h[1])) / ((h[-2] + h[-1] + h[0]) * (h[-2] + h[-1]));
+   const double D3 = h[-2] + 2.0 * h[-1];
+   const realf V3a = (realf)((double)u[-1] * D3) - (u[-2] * h[-1]);
+   const realf V3 = F2 * V3a;
+   const realf F3 = h[-1] * (h[-2] + h[-1]) / ((h[-1] + h[0] + h[1]) * (h[0] + h[1]));
+   const double D4 = 2.0 * h[0] + h[1];
+   const realf V4a = (realf)((double)u[0] * D4) - u[1] * h[0];
+   const realf V4 = F3 * V4a;
+   const realf S = V2 + V3 + V4;
+   return (realf)(D1 * (double)S);
+}
+
+static void ppm_coeff_nonuniform(const realf* h, const realf* v, realf threshold, realf a[3]) {
+   realf fl = h4_face_nonuniform(h, v);
+   realf fr = h4_face_nonuniform(h + 1, v + 1);
+   realf slope_abs, slope_sign;
+   if (threshold > 0) {
+      const realf scale = (realf)(1.0 / (double)threshold);
+      const realf s = superbee(v[-1] * scale, v[0] * scale, v[1] * scale);
+      slope_abs = (realf)fabs(s) * threshold;
+      slope_sign = (s > 0) ? (realf)1 : (realf)-1;
+   } else {
+      const realf s = superbee(v[-1], v[0], v[1]);
+      slope_abs = (realf)fabs(s);
+      slope_sign = (s > 0) ? (realf)1 : (realf)-1;
+   }
+   if (slope_abs == (realf)0) { fr = v[0]; fl = v[0]; }
+   if ((v[-1] - fl) * (fl - v[0]) < 0) fl = v[0] - (realf)(slope_sign * 0.5) * slope_abs;
+   if ((v[1] - fr) * (fr - v[0]) < 0) fr = v[0] + (realf)(slope_sign * 0.5) * slope_abs;
+   const realf one_sixth = (realf)(1.0 / 6.0);
+   {
+      const realf d = fr - fl, e = v[0] - (realf)(0.5 * (fl + fr));
+      if (d * e > d * d * one_sixth) fl = (realf)3 * v[0] - (realf)2 * fr;
+   }
+   {
+      const realf d = fr - fl, e = v[0] - (realf)(0.5 * (fl + fr));
+      if (-d * d * one_sixth > d * e) fr = (realf)3 * v[0] - (realf)2 * fl;
+   }
+   a[0] = fl;
+   a[1] = (realf)(3.0 * v[0]) - (realf)(2.0 * fl) - fr;
+   a[2] = fl + fr - (realf)(2.0 * v[0]);
+}
+
+int orc_translate(const orc_mesh* m, const uint32_t grid[3], const uint64_t* offsets, const uint32_t* gids,
+                  const realf* data, uint32_t dim, realf dt, realf dz, double min_value, realf* data_out) {
+   if (dim > 2) return ORC_EINVAL;
+   const uint32_t nx = grid[0], ny = grid[1], nz = grid[2];
+   const uint64_t ncells = (uint64_t)nx * ny * nz;
+   const uint32_t N = grid[dim];
+   const size_t nb = (size_t)m->len[0] * m->len[1] * m->len[2];
+   const realf dvz = (realf)mesh_dv(m, (int)dim);
+   const realf vz_min = (realf)m->vmin[dim];
+   const realf threshold = (realf)min_value;
+   /* stride between consecutive cells along dim */
+   const uint64_t stride = dim == 0 ? 1 : (dim == 1 ? nx : (uint64_t)nx * ny);
+   const uint32_t n_other = (uint32_t)(ncells / N);
+   int32_t* where = (int32_t*)malloc(sizeof(int32_t) * nb * N);
+   unsigned char* inunion = (unsigned char*)malloc(nb);
+   realf* vals = (realf*)malloc(sizeof(realf) * (size_t)N * WID3);
+   realf* outv = (realf*)malloc(sizeof(realf) * (size_t)N * WID3);
+   realf* hbuf = (realf*)malloc(sizeof(realf) * (N + 8));
+   if (!where || !inunion || !vals || !outv || !hbuf) {
+      free(where); free(inunion); free(vals); free(outv); free(hbuf);
+      return ORC_ENOMEM;
+   }
+   for (uint32_t q = 0; q < N + 8; ++q) hbuf[q] = dz;
+   const realf* h = hbuf + 4; /* h[-4 .. N+3] */
+   memcpy(data_out, data, sizeof(realf) * WID3 * (size_t)offsets[ncells]);
+   for (uint32_t p = 0; p < n_other; ++p) {
+      /* first cell of this pencil */
+      uint64_t c0;
+      if (dim == 0) c0 = (uint64_t)p * nx;
+      else if (dim == 1) c0 = (uint64_t)(p % nx) + (uint64_t)nx * ny * (p / nx);
+      else c0 = p;
+      memset(inunion, 0, nb);
+      for (uint32_t x = 0; x < N; ++x) {
+         const uint64_t c = c0 + x * stride;
+         for (size_t g = 0; g < nb; ++g) where[(size_t)x * nb + g] = -1;
+         for (uint64_t b = offsets[c]; b < offsets[c + 1]; ++b) {
+            where[(size_t)x * nb + gids[b]] = (int32_t)b;
+            inunion[gids[b]] = 1;
+         }
+      }
+      for (size_t g = 0; g < nb; ++g) {
+         if (!inunion[g]) continue;
+         for (uint32_t x = 0; x < N; ++x) {
+            const int32_t b = where[(size_t)x * nb + g];
+            for (int q = 0; q < WID3; ++q) vals[(size_t)x * WID3 + q] = b >= 0 ? data[(size_t)b * WID3 + q] : 0;
+            memset(outv + (size_t)x * WID3, 0, sizeof(realf) * WID3);
+         }
+         uint32_t s[3];
+         swapped_indices((uint32_t)g, m, (int)dim, s);
+         for (uint32_t i = 0; i < N; ++i) {
+            const uint32_t im1 = (i + N - 1) % N, ip1 = (i + 1) % N;
+            for (int k = 0; k < WID; ++k) {
+               const realf cell_vz = (realf)((s[2] * WID + k + 0.5) * (double)dvz + (double)vz_min);
+               const realf zt = cell_vz * dt / h[i];
+               const int pos = zt > 0;
+               const realf z_1 = pos ? (realf)(1.0 - zt) : (realf)0;
+               const realf z_2 = pos ? (realf)1 : -zt;
+               /* the reference skips a whole 16-lane plane when no value in the
+                  5-cell stencil is positive (check_skip_remapping) */
+               int any_pos = 0;
+               for (int di = -2; di <= 2 && !any_pos; ++di) {
+                  const uint32_t ii = (uint32_t)(((int)i + di + 2 * (int)N) % (int)N);
+                  for (int lane = 0; lane < WID2; ++lane)
+                     if (vals[(size_t)ii * WID3 + cell_offset((int)dim, lane % WID, lane / WID, k)] > 0) {
+                        any_pos = 1;
+                        break;
+                     }
+               }
+               if (!any_pos) continue;
+               for (int lane = 0; lane < WID2; ++lane) {
+                  const int off = cell_offset((int)dim, lane % WID, lane / WID, k);
+                  realf st[5];
+                  for (int di = -2; di <= 2; ++di) {
+                     const uint32_t ii = (uint32_t)(((int)i + di + 2 * (int)N) % (int)N);
+                     st[di + 2] = vals[(size_t)ii * WID3 + off];
+                  }
+                  realf a[3];
+                  ppm_coeff_nonuniform(h + i, st + 2, threshold, a);
+                  const realf ngbr = z_2 * (a[0] + z_2 * (a[1] + z_2 * a[2])) - z_1 * (a[0] + z_1 * (a[1] + z_1 * a[2]));
+                  if (where[(size_t)i * nb + g] >= 0) {
+                     realf* t = outv + (size_t)i * WID3 + off;
+                     *t = *t + (st[2] - ngbr) * (realf)1;
+                  }
+                  if (where[(size_t)ip1 * nb + g] >= 0) {
+                     realf* t = outv + (size_t)ip1 * WID3 + off;
+                     *t = *t + (pos ? ngbr * h[i] / h[i + 1] : (realf)0) * (realf)1;
+                  }
+                  if (where[(size_t)im1 * nb + g] >= 0) {
+                     realf* t = outv + (size_t)im1 * WID3 + off;
+                     *t = *t + (!pos ? ngbr * h[i] / h[(int)i - 1] : (realf)0) * (realf)1;
+                  }
+               }
+            }
+         }
+         for (uint32_t x = 0; x < N; ++x) {
+            const int32_t b = where[(size_t)x * nb + g];
+            if (b >= 0) memcpy(data_out + (size_t)b * WID3, outv + (size_t)x * WID3, sizeof(realf) * WID3);
+         }
+      }
+   }
+   free(where); free(inunion); free(vals); free(outv); free(hbuf);
+   return ORC_OK;
+}

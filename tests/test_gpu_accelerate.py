@@ -1,0 +1,131 @@
+"""Parity of the full CUDA acceleration step with the oracle.
+
+One step = FP64 moments (pivot) -> FP64 gyration transform and SLICE-3D
+intersections -> three sweeps -> block adjustment -> moments with pressure,
+i.e. calculateAcceleration for one population and one subcycle
+(vlasovsolver/vlasovmover.cpp:410-475, 564-569).
+
+Tolerances: the FP64 geometry on the device and on the host may differ in the
+last bits (library sin/cos), so intersections are compared to 1e-12 relative;
+wherever the intersections agree after conversion to Realf the VDF and block
+set must be bit-identical; moments agree to 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from vlasiator_b200.mesh import CHARGE, MASS_PROTON, WID3
+from vlasiator_b200.projects import larmor_cell, random_drifting_cells
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def vl():
+    from vlasiator_b200 import vlgpu
+    vlgpu.load()
+    return vlgpu
+
+
+def _run_gpu(vl, mesh, cells, dt, map_order, per_cell=False):
+    total = sum(c.n_blocks for c in cells)
+    with vl.Batch(mesh, len(cells), 3 * total + 65536) as b:
+        b.upload([c.gids for c in cells], [c.data for c in cells])
+        if per_cell:
+            b.accelerate(np.stack([c.B for c in cells]), dt, map_order)  # stages fields on the device
+            b.upload([c.gids for c in cells], [c.data for c in cells])
+            b.accelerate_device(map_order, per_cell=True)
+        else:
+            b.accelerate(np.stack([c.B for c in cells]), dt, map_order)
+        out = dict(cells=b.cells(), isect=b.intersections(), status=b.status(), loss=b.rho_loss(),
+                   moments=b.moments(second=True))
+    return out
+
+
+def _dt(cells, frac):
+    return np.array([frac * 2 * np.pi * MASS_PROTON / (CHARGE * np.linalg.norm(c.B)) for c in cells])
+
+
+def test_full_step_matches_oracle(vl, mesh, orc_sp):
+    cells = random_drifting_cells(32, seed=21)
+    dt = _dt(cells, 0.01)
+    mo = 2
+    got = _run_gpu(vl, mesh, cells, dt, mo)
+    assert not got["status"].any()
+    exact = 0
+    for ci, c in enumerate(cells):
+        g, d, isect, loss, mom, wall = orc_sp.accelerate_step(mesh, c.gids, c.data, c.B, dt[ci], mo, MASS_PROTON,
+                                                              CHARGE)
+        np.testing.assert_allclose(got["isect"][ci], isect, rtol=1e-12, atol=1e-9)
+        g1, d1 = got["cells"][ci]
+        if np.array_equal(got["isect"][ci].astype(np.float32), isect.astype(np.float32)):
+            np.testing.assert_array_equal(g1, g, err_msg=f"cell {ci}")
+            assert np.array_equal(d1, d), f"cell {ci}: VDF not bit-exact"
+            exact += 1
+        else:
+            peak = float(np.abs(d).max())
+            common = np.intersect1d(g1, g)
+            assert abs(len(g1) - len(g)) <= 0.01 * len(g) + 2
+            i1, i2 = np.searchsorted(g1, common), np.searchsorted(g, common)
+            assert np.abs(d1[i1] - d[i2]).max() <= 1e-5 * peak
+        m1 = got["moments"][ci]
+        np.testing.assert_allclose(m1[[0, 4, 8, 15]], mom[[0, 4, 8, 15]], rtol=1e-10)
+        np.testing.assert_allclose(m1[5:8], mom[5:8], rtol=1e-9, atol=1e-6)
+        scale = np.abs(mom[9:12]).max()
+        np.testing.assert_allclose(m1[9:15], mom[9:15], rtol=1e-9, atol=1e-10 * scale)
+        assert got["loss"][ci] == pytest.approx(loss, rel=1e-9, abs=1e-30)
+    assert exact >= len(cells) - 1
+
+
+def test_mass_conservation_and_larmor_gyration(vl, mesh):
+    """Pure gyration about B through V = 0: mass is conserved to 1e-6 per step
+    (up to the block-adjust loss, which is accounted) and |v|-moments stay put."""
+    c = larmor_cell()
+    dt = _dt([c], 0.01)
+    with vl.Batch(mesh, 1, 65536) as b:
+        b.upload([c.gids], [c.data])
+        m0 = b.moments(second=True)[0]
+        for step in range(10):
+            b.accelerate(c.B[None, :], dt, step % 3)
+        m1 = b.moments(second=True)[0]
+        loss = b.rho_loss()[0]
+        assert not b.status().any()
+    assert abs((m1[0] + loss) / m0[0] - 1.0) < 1e-5          # 10 steps, 1e-6 each
+    assert abs(m1[9] + m1[10] - m0[9] - m0[10]) / (m0[9] + m0[10]) < 2e-2  # perpendicular pressure
+    assert abs(m1[11] / m0[11] - 1.0) < 1e-3                  # parallel pressure unchanged
+
+
+def test_plain_per_cell_path_equals_batched(vl, mesh):
+    cells = random_drifting_cells(10, seed=33)
+    dt = _dt(cells, 0.02)
+    a = _run_gpu(vl, mesh, cells, dt, 1)
+    b = _run_gpu(vl, mesh, cells, dt, 1, per_cell=True)
+    for (g1, d1), (g2, d2) in zip(a["cells"], b["cells"]):
+        np.testing.assert_array_equal(g1, g2)
+        assert np.array_equal(d1, d2)
+    np.testing.assert_array_equal(a["moments"], b["moments"])
+
+
+def test_adjust_matches_oracle(vl, mesh, orc_sp):
+    """Adjustment straight after upload (content computed from the data)."""
+    cells = random_drifting_cells(8, seed=44)
+    rng = np.random.default_rng(1)
+    gl, dl = [], []
+    for c in cells:
+        # drop a few blocks and add some empty ones so that adjustment has work
+        keep = rng.random(c.n_blocks) > 0.05
+        extra = np.setdiff1d(rng.integers(0, mesh.max_blocks, 50).astype(np.uint32), c.gids)
+        g = np.concatenate([c.gids[keep], extra])
+        d = np.concatenate([c.data[keep], np.full((len(extra), WID3), 3e-16, np.float32)])
+        o = np.argsort(g)
+        gl.append(g[o])
+        dl.append(d[o])
+    with vl.Batch(mesh, len(cells), 200000) as b:
+        b.upload(gl, dl)
+        b.adjust()
+        got = b.cells()
+        loss = b.rho_loss()
+    for ci in range(len(cells)):
+        g, d, l_ = orc_sp.adjust(mesh, gl[ci], dl[ci], 1e-15)
+        np.testing.assert_array_equal(got[ci][0], g)
+        assert np.array_equal(got[ci][1], d)
+        assert loss[ci] == pytest.approx(l_, rel=1e-12)

@@ -93,9 +93,10 @@ struct vlgpu_batch {
    uint32_t* status = nullptr;
    SweepCounters* counters = nullptr;
    BatchStats* stats = nullptr;
-   // pinned staging
+   // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;
    CellAccelInputs* h_accel = nullptr;
+   cudaEvent_t ev_sweep = nullptr, ev_accel = nullptr;
    // host-side accounting
    unsigned long long launches = 0;
    unsigned long long remap_launches = 0;
@@ -144,6 +145,8 @@ void free_batch(vlgpu_batch* b) {
    for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
    cudaFreeHost(b->h_sweep);
    cudaFreeHost(b->h_accel);
+   if (b->ev_sweep) cudaEventDestroy(b->ev_sweep);
+   if (b->ev_accel) cudaEventDestroy(b->ev_accel);
    if (b->stream) cudaStreamDestroy(b->stream);
    delete b;
 }
@@ -211,10 +214,12 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
 
 // One sweep with host-given intersections (4 doubles per cell at `stride`).
 int run_sweep(vlgpu_batch* b, const double* intersections, size_t stride, uint32_t dim, bool per_cell) {
+   VL_CHECK(cudaEventSynchronize(b->ev_sweep));  // the previous copy out of h_sweep has been read
    for (uint32_t c = 0; c < b->n_cells; ++c)
       b->h_sweep[c] = make_sweep_cell(intersections + stride * c, dim, b->params.min_value);
    VL_CHECK(cudaMemcpyAsync(b->sweep_cells, b->h_sweep, sizeof(SweepCell) * b->n_cells, cudaMemcpyHostToDevice,
                             b->stream));
+   VL_CHECK(cudaEventRecord(b->ev_sweep, b->stream));
    return sweep_device(b, b->sweep_cells, dim, per_cell, false);
 }
 
@@ -259,7 +264,8 @@ int materialize(vlgpu_batch* b) {
    return VLGPU_OK;
 }
 
-int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
+// Pivot moments and the per-cell FP64 geometry of one acceleration step.
+int geometry_device(vlgpu_batch* b, uint32_t map_order) {
    // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420)
    int st = moments_device(b, false);
    if (st != VLGPU_OK) return st;
@@ -267,6 +273,12 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
    VL_CHECK(launch_geometry(b->accel_in, b->moments, b->isect12, b->sweep3, b->n_cells, b->params.charge,
                             b->params.mass, b->params.hall_minimum_rhoq, (int)b->params.ohm_gradpe, MU_0, b->vmin_d,
                             b->dv_d, map_order, (float)b->params.min_value, b->stream));
+   return VLGPU_OK;
+}
+
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
+   int st = geometry_device(b, map_order);
+   if (st != VLGPU_OK) return st;
    static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
    for (int s = 0; s < 3; ++s) {
       const uint32_t d = orders[map_order][s];
@@ -280,6 +292,7 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
 }
 
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
+   VL_CHECK(cudaEventSynchronize(b->ev_accel));  // the previous copy out of h_accel has been read
    for (uint32_t c = 0; c < b->n_cells; ++c) {
       CellAccelInputs& a = b->h_accel[c];
       for (int r = 0; r < 3; ++r) {
@@ -291,6 +304,7 @@ int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* 
    }
    VL_CHECK(cudaMemcpyAsync(b->accel_in, b->h_accel, sizeof(CellAccelInputs) * b->n_cells, cudaMemcpyHostToDevice,
                             b->stream));
+   VL_CHECK(cudaEventRecord(b->ev_accel, b->stream));
    return VLGPU_OK;
 }
 
@@ -365,6 +379,8 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMemset(b->stats, 0, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMallocHost(&b->h_sweep, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "pinned");
    if ((e = cudaMallocHost(&b->h_accel, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "pinned");
+   if ((e = cudaEventCreateWithFlags(&b->ev_sweep, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+   if ((e = cudaEventCreateWithFlags(&b->ev_accel, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
    set_direct_state(b, 0);
    *out = b;
    return VLGPU_OK;
@@ -517,6 +533,15 @@ int vlgpu_accelerate(vlgpu_batch* b, const vlgpu_cell_fields* fields, const doub
    int st = stage_fields(b, fields, dt);
    if (st != VLGPU_OK) return st;
    return accelerate_device(b, map_order, false);
+}
+
+int vlgpu_compute_intersections(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt,
+                                uint32_t map_order) {
+   if (!b || !fields || !dt || map_order > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   int st = stage_fields(b, fields, dt);
+   if (st != VLGPU_OK) return st;
+   return geometry_device(b, map_order);
 }
 
 int vlgpu_accelerate_device(vlgpu_batch* b, uint32_t map_order) {

@@ -215,9 +215,8 @@ __global__ void geometry_kernel(const CellAccelInputs* __restrict__ in, const do
    const geom::Affine T = geom::acceleration_transform(ti);
    const double mn[3] = {vmin0, vmin1, vmin2};
    const double dv[3] = {dv0, dv1, dv2};
-   double I[12];
+   double* I = isect12 + (size_t)c * 12;
    geom::cell_intersections(T, mn, dv, map_order, I);
-   for (int r = 0; r < 12; ++r) isect12[(size_t)c * 12 + r] = I[r];
    for (int d = 0; d < 3; ++d) {
       SweepCell s;
       float di = (float)I[4 * d + 1], dj = (float)I[4 * d + 2], dk = (float)I[4 * d + 3];

@@ -70,6 +70,7 @@ SIGNATURES = {
     "vlgpu_accelerate_with_intersections": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
     "vlgpu_accelerate": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), _dp, ctypes.c_uint32]),
     "vlgpu_accelerate_device": (ctypes.c_int, [_vp, ctypes.c_uint32]),
+    "vlgpu_compute_intersections": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), _dp, ctypes.c_uint32]),
     "vlgpu_accelerate_per_cell": (ctypes.c_int, [_vp, ctypes.c_uint32]),
     "vlgpu_adjust_blocks": (ctypes.c_int, [_vp]),
     "vlgpu_batch_rho_loss": (ctypes.c_int, [_vp, _dp]),
@@ -219,8 +220,26 @@ class Batch:
         _check(self.lib.vlgpu_accelerate_with_intersections(self.h, _p(I, ctypes.c_double), map_order),
                "vlgpu_accelerate_with_intersections")
 
+    def _fields(self, B, dt, curl, egradpe):
+        n = self.n_cells
+        F = (CFieldsT * n)()
+        B = np.asarray(B, np.float64).reshape(n, 3)
+        curl = np.zeros((n, 3)) if curl is None else np.asarray(curl, np.float64).reshape(n, 3)
+        eg = np.zeros((n, 3)) if egradpe is None else np.asarray(egradpe, np.float64).reshape(n, 3)
+        for c in range(n):
+            for r in range(3):
+                F[c].B[r], F[c].curl[r], F[c].egradpe[r] = B[c, r], curl[c, r], eg[c, r]
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (n,)))
+        return F, dt
+
+    def compute_intersections(self, B, dt, map_order: int, curl=None, egradpe=None) -> np.ndarray:
+        F, dt = self._fields(B, dt, curl, egradpe)
+        _check(self.lib.vlgpu_compute_intersections(self.h, F, _p(dt, ctypes.c_double), map_order),
+               "vlgpu_compute_intersections")
+        return self.intersections()
+
     def accelerate(self, B, dt, map_order: int, curl=None, egradpe=None):
-        """One acceleration step (moments -> FP64 geometry -> three sweeps) of every cell."""
+        """One acceleration step (moments -> FP64 geometry -> sweeps -> adjust -> moments) of every cell."""
         n = self.n_cells
         F = (CFieldsT * n)()
         B = np.asarray(B, np.float64).reshape(n, 3)
