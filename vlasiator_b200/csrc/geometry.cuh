@@ -143,29 +143,34 @@ VLGPU_HD inline void add3(const double a[3], const double b[3], double out[3]) {
 VLGPU_HD inline void copy3(const double a[3], double out[3]) {
    for (int r = 0; r < 3; ++r) out[r] = a[r];
 }
+// Component i (0..2, known only at run time) of a 3-vector, read with
+// selects so that no local array is indexed dynamically on the device.
+VLGPU_HD inline double comp(const double v[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 VLGPU_HD inline void store4(const double p000[3], const double p100[3], const double p010[3], const double p001[3],
                             int d, double out[4]) {
-   out[0] = p000[d];
-   out[1] = p100[d] - p000[d];
-   out[2] = p010[d] - p000[d];
-   out[3] = p001[d] - p000[d];
+   out[0] = comp(p000, d);
+   out[1] = comp(p100, d) - comp(p000, d);
+   out[2] = comp(p010, d) - comp(p000, d);
+   out[3] = comp(p001, d) - comp(p000, d);
+}
+
+VLGPU_HD inline void unit(int i, double scale, double out[3]) {
+   for (int r = 0; r < 3; ++r) out[r] = (r == i) ? scale : 0.0;
 }
 
 // first intersections: Euclidian lines along d meet Lagrangian planes
 VLGPU_HD inline void isect_1st(const Affine& bwd, const double mn[3], const double dv[3], int d, double out[4]) {
-   double e[3] = {0, 0, 0};
-   e[d] = 1.0;
-   double pn[3], pp[3], q[3] = {0, 0, 0};
+   double e[3], pn[3], pp[3], q[3], lp[3];
+   unit(d, 1.0, e);
    mat_vec(bwd.L, e, pn);
-   q[d] = mn[d];
+   unit(d, comp(mn, d), q);
    apply(bwd, q, pp);
-   double lp[3];
    for (int r = 0; r < 3; ++r) lp[r] = (r == d) ? 0.0 : 0.5 * dv[r] + mn[r];
    double p000[3], p[3][3];
    line_plane(lp, e, pp, pn, p000);
    for (int a = 0; a < 3; ++a) {
-      double s[3] = {0, 0, 0}, step[3], t[3];
-      s[a] = dv[a];
+      double s[3], step[3], t[3];
+      unit(a, comp(dv, a), s);
       if (a == d) {
          mat_vec(bwd.L, s, step);
          add3(pp, step, t);
@@ -182,21 +187,18 @@ VLGPU_HD inline void isect_1st(const Affine& bwd, const double mn[3], const doub
 // planes normal to n
 VLGPU_HD inline void isect_2nd(const Affine& bwd, const double mn[3], const double dv[3], int d, double out[4]) {
    const int n = (d + 1) % 3;
-   double pn[3] = {0, 0, 0}, pp[3] = {0, 0, 0};
-   pn[n] = 1.0;
-   pp[n] = mn[n] + dv[n] * 0.5;
-   double en[3] = {0, 0, 0}, ld[3];
-   en[n] = 1.0;
+   double pn[3], pp[3], en[3], ld[3], q[3], lp[3];
+   unit(n, 1.0, pn);
+   unit(n, comp(mn, n) + comp(dv, n) * 0.5, pp);
+   unit(n, 1.0, en);
    mat_vec(bwd.L, en, ld);
-   double q[3];
    for (int r = 0; r < 3; ++r) q[r] = (r == d) ? mn[r] : 0.5 * dv[r] + mn[r];
-   double lp[3];
    apply(bwd, q, lp);
    double p000[3], p[3][3];
    line_plane(lp, ld, pp, pn, p000);
    for (int a = 0; a < 3; ++a) {
-      double s[3] = {0, 0, 0}, step[3], t[3];
-      s[a] = dv[a];
+      double s[3], step[3], t[3];
+      unit(a, comp(dv, a), s);
       if (a == n) {
          add3(pp, s, t);
          line_plane(lp, ld, t, pn, p[a]);
@@ -223,7 +225,10 @@ VLGPU_HD inline void isect_3rd(const Affine& bwd, const double mn[3], const doub
    store4(p000, p[0], p[1], p[2], d, out);
 }
 
-// 12 doubles ordered x(4), y(4), z(4), each (intersection, di, dj, dk)
+// 12 doubles ordered x(4), y(4), z(4), each (intersection, di, dj, dk).
+// On the device every run-time component index goes through selects (comp,
+// unit): indexing a local array initialised from kernel parameters with a
+// run-time index produced wrong values with this toolchain.
 VLGPU_HD inline void cell_intersections(const Affine& fwd, const double mn[3], const double dv[3], uint32_t map_order,
                                         double out12[12]) {
    Affine bwd;
