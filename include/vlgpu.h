@@ -109,6 +109,40 @@ int vlgpu_map_1d(vlgpu_batch* b, const double* intersections, uint32_t dimension
    drop-in path, vlasovsolver/cpu_acc_semilag.cpp:64-75 without OpenMP). */
 int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t dimension);
 
+/* The same sweep for callers that must not allocate device memory.  It has no
+   counterpart in the reference: it exists for host codes that reserve all of
+   the GPU's memory for their own pool at start-up, and for codes that call
+   the sweep on a latency-critical path, where a cudaMalloc/cudaFree would
+   synchronise the whole device.  It allocates nothing: its work arrays live
+   in one fixed device array of about 3.3 MB inside libvlgpu.so, held by every
+   GPU that loads the library until the process exits.
+   Limits per call: 1..VLGPU_NOALLOC_MAX_CELLS cells, input block indices
+   below VLGPU_NOALLOC_MAX_BLOCKS (offsets[n_cells] <= the limit) and at most
+   VLGPU_NOALLOC_MAX_BLOCKS output blocks; larger inputs are rejected with
+   VLGPU_EINVAL and a message on stderr, an output that does not fit with
+   VLGPU_ENOMEM.
+   Inputs: cell c owns blocks offsets[c] .. offsets[c+1]-1 (host array of
+   n_cells+1) of gids_in / data_in (device memory, 64 floats per block, block
+   IDs inside the mesh); intersections as for vlgpu_map_1d (host).  Outputs:
+   gids_out / data_out (device memory, room for out_capacity blocks); cell c's
+   blocks are cell_off[c] .. cell_off[c]+cell_count[c]-1 of them, in sweep
+   order (host arrays of n_cells); status (host, may be NULL) gets each cell's
+   VLGPU_CELL_* bits of this call.  data_in and data_out are 16-byte aligned.
+   The work is issued on `stream` (a cudaStream_t of the current device, NULL
+   for the default stream) and the call synchronises it before returning.
+   The first call on a device, with that device current, looks up the device
+   array's address (cudaGetSymbolAddress); make that first call before any
+   stream capture begins.  Every call on a device uses the same array: calls
+   that overlap on the GPU (from several host threads at once) race and must
+   be serialised by the caller. */
+#define VLGPU_NOALLOC_MAX_BLOCKS 65536u
+#define VLGPU_NOALLOC_MAX_CELLS 1024u
+int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* params, uint32_t n_cells,
+                         const uint64_t* offsets, const uint32_t* gids_in, const float* data_in,
+                         const double* intersections, uint32_t dimension, uint32_t* gids_out, float* data_out,
+                         uint64_t out_capacity, uint32_t* cell_off, uint32_t* cell_count, uint32_t* status,
+                         void* stream);
+
 /* Three sweeps in map_order 0 (XYZ), 1 (YZX) or 2 (ZXY) with given
    intersections (12 doubles per cell ordered x, y, z; cpu_accelerate_cell,
    vlasovsolver/cpu_acc_semilag.cpp:92-130). */

@@ -82,6 +82,9 @@ SIGNATURES = {
     "vlgpu_batch_stats2": (ctypes.c_int, [_vp, _u64p]),
     "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
+    "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
+                                            _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
+                                            _u32p, _vp]),
     "vlgpu_version": (ctypes.c_char_p, []),
 }
 
