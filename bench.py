@@ -41,6 +41,11 @@ METRIC = "phase-space cell-updates/s (batched vs plain, same GPU); p50/p99 solve
 UNIT = "cell-updates/s"
 WORKLOAD = "batched acceleration, 4096 drifting Maxwellian cells, 1 SLICE-3D step (PPM), dt=0.01 gyroperiod"
 BYTES_PER_CELL_SWEEP = 8  # read + write one fp32 phase-space cell per 1D sweep
+# DRAM bytes (read + write) of one remap launch per source block, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 381.0 MB) of the
+# 512-cell case of this workload (705,499 blocks), fused arithmetic; scaled by
+# the source blocks of a launch to give the full-size traffic per launch.
+REMAP_DRAM_BYTES_PER_BLOCK = 381.0e6 / 705499
 
 
 def workload(n_cells: int, seed: int):
@@ -236,7 +241,7 @@ def run_ours(args):
     orders = map_orders(args.warmup + args.steps, args.seed)
     total = int(offs[-1])
     cap = int(total * 1.6) + 262144
-    batch = vlgpu.Batch(mesh, args.cells, cap, device=local)
+    batch = vlgpu.Batch(mesh, args.cells, cap, device=local, exact=args.exact)
     batch.upload_packed(offs, gids, data)
     stream = torch.cuda.ExternalStream(batch.stream_handle(), device=local)
 
@@ -250,16 +255,16 @@ def run_ours(args):
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with ClockSampler(local) as clk:
-        ev0.record(stream)
+        evs[0].record(stream)
         for s in range(args.steps):
             batch.accelerate_device(orders[args.warmup + s])
-        ev1.record(stream)
-        ev1.synchronize()
+            evs[s + 1].record(stream)
+        evs[-1].synchronize()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    ms = evs[0].elapsed_time(evs[-1])
+    step_ms = np.array([evs[q].elapsed_time(evs[q + 1]) for q in range(args.steps)])
     st1 = batch.stats()
     status = batch.status()
     updates = WID3 * (st1["step_blocks"] - st0["step_blocks"])
@@ -273,6 +278,28 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     achieved = (BYTES_PER_CELL_SWEEP * WID3 * src_blocks / remap_n) / (remap_ms * 1e-3 / remap_n) / 1e9 \
         if remap_n else None
+
+    # the plain per-cell launch path (the drop-in baseline) on the same batch
+    plain = None
+    if args.plain_steps > 0:
+        batch.profile(False)
+        batch.upload_packed(offs, gids, data)
+        p_steps = max(1, min(args.steps, args.plain_steps))
+        pst0 = batch.stats()
+        pe0 = torch.cuda.Event(enable_timing=True)
+        pe1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        pe0.record(stream)
+        for s in range(p_steps):
+            batch.accelerate_device(orders[args.warmup + s], per_cell=True)
+        pe1.record(stream)
+        pe1.synchronize()
+        p_ms = allreduce_max(pg, pe0.elapsed_time(pe1))
+        p_upd = allreduce_sum(pg, float(WID3 * (batch.stats()["step_blocks"] - pst0["step_blocks"])))
+        p_value = p_upd / (p_ms * 1e-3)
+        plain = {"value": p_value, "unit": UNIT, "steps": p_steps, "ms_per_step": p_ms / p_steps,
+                 "batched_over_plain": value / p_value,
+                 "path": "vlgpu_accelerate_per_cell: one columnize + remap launch sequence per cell and sweep"}
 
     # end to end through the C ABI: host -> device copy of the step's input,
     # the step, device -> host copy of the result (pinned host buffers)
@@ -313,10 +340,17 @@ def run_ours(args):
                    "mean_blocks_per_cell": total / args.cells, "l2": "inputs larger than L2 (126 MB)",
                    "parallelism": f"{world} independent batches (no data-path collective)"},
         "gpu_launches": launches,
+        "arithmetic": "exact (bit-identical to the reference's map_1d)" if args.exact else
+                      "fused (reference PPM, FMA target distribution; 1e-5 of peak per step)",
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                       "what": "device time of one batched acceleration step of all cells"},
+        "plain_per_cell": plain,
         "status_cells_flagged": int((status != 0).sum()),
         "roofline": {"bound": "hbm", "kernel": "remap_kernel", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": (REMAP_DRAM_BYTES_PER_BLOCK * src_blocks / remap_n) if remap_n else None,
+                     "traffic_note": "bytes per launch, ncu capture of the 512-cell case scaled by source blocks",
                      "algorithmic_bytes": "8 B per source phase-space cell per sweep"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(e2e_steps, 1),
                 "d2h_bytes_per_step": d2h // max(e2e_steps, 1), "steps": e2e_steps,
@@ -342,6 +376,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--ref-sample", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--exact", action="store_true", help="remap in the reference's exact operation order")
+    ap.add_argument("--plain-steps", type=int, default=2, help="steps of the plain per-cell path (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

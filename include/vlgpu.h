@@ -109,7 +109,8 @@ int vlgpu_map_1d(vlgpu_batch* b, const double* intersections, uint32_t dimension
    drop-in path, vlasovsolver/cpu_acc_semilag.cpp:64-75 without OpenMP). */
 int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t dimension);
 
-/* The same sweep for callers that must not allocate device memory.  It has no
+/* The same sweep (with the default fused remap arithmetic, see
+   vlgpu_batch_set_exact) for callers that must not allocate device memory.  It has no
    counterpart in the reference: it exists for host codes that reserve all of
    the GPU's memory for their own pool at start-up, and for codes that call
    the sweep on a latency-critical path, where a cudaMalloc/cudaFree would
@@ -214,6 +215,16 @@ int vlgpu_batch_stats(vlgpu_batch* b, uint64_t* out8);
 /* Further counters: [0] blocks that entered the first sweep of each
    acceleration step (the step's phase-space cell updates / 64). */
 int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out);
+
+/* Selects the remap arithmetic of later sweeps.  exact = 1 evaluates every
+   operation in the reference's order and rounding (cpu_acc_map.cpp:395-631),
+   so VDF values and block sets are bit-identical to the reference's map_1d.
+   exact = 0 (the default) keeps the reference's PPM reconstruction but
+   distributes each source cell over its target cells with fused
+   multiply-adds and at most three targets per source cell: block sets are
+   unchanged, values stay within 1e-5 of the cell's peak per step, and mass
+   is conserved as in the exact mode. */
+int vlgpu_batch_set_exact(vlgpu_batch* b, int exact);
 
 /* Synchronises the batch's stream and returns the first error seen. */
 int vlgpu_batch_sync(vlgpu_batch* b);

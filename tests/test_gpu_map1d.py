@@ -1,10 +1,12 @@
 """Parity of the CUDA SLICE-3D sweep (libvlgpu.so, through its C ABI) with the
 reference's map_1d.
 
-The CUDA path evaluates the reference's arithmetic operation by operation, so
-the comparisons below are bit-exact: identical sorted block-ID sets and
-identical float values, against the committed reference fixtures and against
-the oracle restatement on seeded random cells.
+In its exact mode (vlgpu_batch_set_exact(1)) the CUDA path evaluates the
+reference's arithmetic operation by operation, so those comparisons are
+bit-exact: identical sorted block-ID sets and identical float values, against
+the committed reference fixtures and against the oracle restatement on seeded
+random cells.  The default fused mode is held to identical block sets and
+values within 1e-5 of each cell's peak per sweep, with mass conserved to 1e-6.
 """
 import os
 
@@ -42,7 +44,7 @@ def test_golden_sweeps_bit_exact(vl, mesh):
         g, d = z[f"{name}/gids_in"], z[f"{name}/data_in"]
         isect = z[f"{name}/isect"]
         mo = int(z[f"{name}/map_order"])
-        with vl.Batch(mesh, 1, 4 * len(g) + 4096) as b:
+        with vl.Batch(mesh, 1, 4 * len(g) + 4096, exact=True) as b:
             b.upload([g], [d])
             for s, dim in enumerate(ORDERS[mo]):
                 b.map_1d(isect[4 * dim:4 * dim + 4][None, :], dim)
@@ -58,7 +60,7 @@ def test_batched_random_cells_bit_exact(vl, mesh, orc_sp):
     mo = 1
     I = np.stack([geometry(orc_sp, c, 0.03, mesh, mo) for c in cells])
     total = sum(c.n_blocks for c in cells)
-    with vl.Batch(mesh, len(cells), 3 * total + 65536) as b:
+    with vl.Batch(mesh, len(cells), 3 * total + 65536, exact=True) as b:
         b.upload([c.gids for c in cells], [c.data for c in cells])
         ref = [(c.gids, c.data) for c in cells]
         for dim in ORDERS[mo]:
@@ -73,13 +75,14 @@ def test_batched_random_cells_bit_exact(vl, mesh, orc_sp):
         assert not b.status().any()
 
 
-def test_per_cell_path_equals_batched(vl, mesh, orc_sp):
+@pytest.mark.parametrize("exact", [True, False])
+def test_per_cell_path_equals_batched(vl, mesh, orc_sp, exact):
     cells = random_drifting_cells(12, seed=9)
     I = np.stack([geometry(orc_sp, c, 0.05, mesh, 2) for c in cells])
     total = sum(c.n_blocks for c in cells)
     outs = []
     for per_cell in (False, True):
-        with vl.Batch(mesh, len(cells), 3 * total + 65536) as b:
+        with vl.Batch(mesh, len(cells), 3 * total + 65536, exact=exact) as b:
             b.upload([c.gids for c in cells], [c.data for c in cells])
             for dim in ORDERS[2]:
                 b.map_1d(I[:, 4 * dim:4 * dim + 4], dim, per_cell=per_cell)
@@ -92,7 +95,7 @@ def test_per_cell_path_equals_batched(vl, mesh, orc_sp):
 def test_three_sweeps_entry_point(vl, mesh, orc_sp):
     c = larmor_cell()
     I = geometry(orc_sp, c, 0.01, mesh, 0)
-    with vl.Batch(mesh, 1, 8192) as b:
+    with vl.Batch(mesh, 1, 8192, exact=True) as b:
         b.upload([c.gids], [c.data])
         b.accelerate_with_intersections(I[None, :], 0)
         (g, d), = b.cells()
@@ -114,7 +117,7 @@ def test_edge_cases(vl, mesh, orc_sp):
     cells_g = [np.zeros(0, np.uint32), single_g, wall.gids]
     cells_d = [np.zeros((0, WID3), np.float32), single_d, wall.data]
     I = np.array([[-4.02e6 + 0.3 * 3e4, 0.0, 0.0, 3e4]] * 3)
-    with vl.Batch(mesh, 3, 65536) as b:
+    with vl.Batch(mesh, 3, 65536, exact=True) as b:
         b.upload(cells_g, cells_d)
         b.map_1d(I, 2)
         got = b.cells()
@@ -126,3 +129,31 @@ def test_edge_cases(vl, mesh, orc_sp):
         assert np.array_equal(got[ci][1], d2)
         assert bool(st[ci] & vl.CELL_WALL) == bool(fl & 1)
     assert st[2] & vl.CELL_WALL
+
+
+@pytest.mark.parametrize("mo", [0, 1, 2])
+def test_fast_sweeps_within_tolerance(vl, mesh, orc_sp, mo):
+    """Default (fused) remap against the oracle, sweep by sweep: identical
+    block sets, values within 1e-5 of the cell's peak, mass to 1e-6."""
+    cells = random_drifting_cells(40, seed=100 + mo)
+    I = np.stack([geometry(orc_sp, c, 0.02, mesh, mo) for c in cells])
+    total = sum(c.n_blocks for c in cells)
+    state = [(c.gids, c.data) for c in cells]
+    with vl.Batch(mesh, len(cells), 3 * total + 65536) as b:
+        assert not b.exact
+        for dim in ORDERS[mo]:
+            # every sweep starts from the oracle's state, so errors do not compound
+            b.upload([g for g, _ in state], [d for _, d in state])
+            b.map_1d(I[:, 4 * dim:4 * dim + 4], dim)
+            got = b.cells()
+            ref = [orc_sp.map_1d(mesh, g, d, I[ci, 4 * dim:4 * dim + 4], dim, 1e-15)[:2]
+                   for ci, (g, d) in enumerate(state)]
+            for ci, ((g1, d1), (g2, d2)) in enumerate(zip(got, ref)):
+                np.testing.assert_array_equal(g1, g2, err_msg=f"cell {ci} dim {dim}")
+                peak = float(np.abs(d2).max())
+                err = float(np.abs(d1 - d2).max())
+                assert err <= 1e-5 * peak, f"cell {ci} dim {dim}: {err / peak:.2e} of peak"
+                m1, m2 = float(d1.astype(np.float64).sum()), float(d2.astype(np.float64).sum())
+                assert abs(m1 / m2 - 1.0) <= 1e-6, f"cell {ci} dim {dim}: mass {m1 / m2 - 1.0:.2e}"
+            assert not b.status().any()
+            state = ref

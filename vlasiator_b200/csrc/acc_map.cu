@@ -48,6 +48,14 @@ __device__ __forceinline__ float h4_face(float vm2, float vm1, float v0, float v
    s = fs(s, vp1);
    return dmf(1.0 / 12.0, s);
 }
+// The same face in single precision throughout (fused mode).
+__device__ __forceinline__ float h4_face_fused(float vm2, float vm1, float v0, float vp1) {
+   return fmaf(7.0f, vm1 + v0, -(vm2 + vp1)) * (float)(1.0 / 12.0);
+}
+template <bool FUSED>
+__device__ __forceinline__ float h4_face_mode(float vm2, float vm1, float v0, float vp1) {
+   return FUSED ? h4_face_fused(vm2, vm1, v0, vp1) : h4_face(vm2, vm1, v0, vp1);
+}
 
 __device__ __forceinline__ float minmod(float s1, float s2) {
    const float slope = (fabsf(s1) < fabsf(s2)) ? s1 : s2;
@@ -96,16 +104,21 @@ __device__ __forceinline__ void ppm_coeff(float vm1, float v0, float vp1, float 
 // ---------------------------------------------------------------------------
 // 96-bit mask helpers
 // ---------------------------------------------------------------------------
+// Word q (0..2) of a mask, chosen with selects so that a mask held in
+// registers is never indexed dynamically (which would move it to local memory).
+__device__ __forceinline__ uint32_t mask_word(const uint32_t m[3], int q) {
+   return q == 0 ? m[0] : (q == 1 ? m[1] : m[2]);
+}
 __device__ __forceinline__ int mask_next_set(const uint32_t m[3], int k) {
    for (; k < 96; k = (k | 31) + 1) {
-      const uint32_t w = m[k >> 5] >> (k & 31);
+      const uint32_t w = mask_word(m, k >> 5) >> (k & 31);
       if (w) return k + __ffs(w) - 1;
    }
    return 96;
 }
 __device__ __forceinline__ int mask_next_clear(const uint32_t m[3], int k) {
    for (; k < 96; k = (k | 31) + 1) {
-      const uint32_t w = (~m[k >> 5]) >> (k & 31);
+      const uint32_t w = (~mask_word(m, k >> 5)) >> (k & 31);
       if (w) return k + __ffs(w) - 1;
    }
    return 96;
@@ -372,6 +385,13 @@ __device__ __forceinline__ int cell_offset(int i, int j, int g) {
 
 constexpr uint32_t NO_BLOCK = 0xffffffffu;  // a block that exists with all-zero data
 
+// Integral of the PPM profile a0 + a1 u + a2 u^2 ... from 0 to u, in the
+// reference's normalisation (cpu_acc_map.cpp:585-590), Horner form with FMA.
+__device__ __forceinline__ float ppm_integral(float u, float a0, float a1, float a2) {
+   return u * fmaf(u, fmaf(u, a2, a1), a0);
+}
+__device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
 template <int DIM>
 __device__ __forceinline__ void load_lane(const float* __restrict__ data, uint32_t idx, int i, int j, float v[4]) {
    if (idx == NO_BLOCK) {
@@ -423,8 +443,8 @@ __device__ __forceinline__ void select_lanes(float lag, int lane, unsigned hmask
    min_lane = vmin ? imin : 0;
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
+template <int DIM, bool EXACT>
+__global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
    const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
    const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
@@ -440,6 +460,8 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
    const int max_len = (int)mesh.len[DIM];
    const float dv = mesh.dv[DIM], v_min = mesh.vmin[DIM];
    const double i_dv = 1.0 / (double)dv;
+   // (double)v >= content_threshold  <=>  v >= the smallest float >= the threshold
+   const float content_thr = __double2float_ru(content_threshold);
 
    for (;;) {
       uint32_t sidx = 0;
@@ -457,6 +479,12 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
       const float im = fa(fa(P.intersection, fm(A, P.di)), fm(B, P.dj));
       float mx, mn;
       set_corners(P, cs.si, cs.sj, mx, mn);
+      // fused mode: each lane walks the reference's target edges
+      // (g+1)*dk + im along the column instead of dividing per cell, and a
+      // source cell covers at most three target cells, which holds while the
+      // Lagrangian cell is wider than half a source cell
+      const float inv_dv = (float)i_dv;
+      const bool fused = !EXACT && dk > 0.55f * dv;
 #pragma unroll
       for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
       int next_flush = mask_next_set(cs.tgt_mask, 0);
@@ -476,8 +504,8 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
             const uint32_t o = cs.dst_pos + out_idx;
             store_lane<DIM>(dst_data + (size_t)o * WID3, i, j, v);
             // content flag of the finished block (compute_block_has_content)
-            const bool c = ((double)v[0] >= content_threshold) | ((double)v[1] >= content_threshold) |
-                           ((double)v[2] >= content_threshold) | ((double)v[3] >= content_threshold);
+            const bool c = (v[0] >= content_thr) | (v[1] >= content_thr) | (v[2] >= content_thr) |
+                           (v[3] >= content_thr);
             const unsigned any_c = __ballot_sync(hmask, c) & hmask;
             if (lane == 0) {
                dst_gids[o] = gid_from_swapped(cs.si, cs.sj, (uint32_t)next_flush, mesh.len, DIM);
@@ -510,6 +538,19 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
             select_lanes(lag, lane, hmask, max_lane, min_lane);
          }
          const int gk_lo_col = cf * WID, gk_hi_col = (cl + 1) * WID - 1;
+         // fused mode: g0 = the lane's first target (edge(g0+1) > v), e1/e2 =
+         // edge(g0+1)/edge(g0+2), gf = g0 as a float
+         int g0 = gk_r - 2;
+         float gf = (float)g0;
+         float e1 = fa(fm(gf + 1.0f, dk), im), e2 = fa(fm(gf + 2.0f, dk), im);
+         if (fused) {
+            for (int q = 0; q < 6 && e1 <= v_r; ++q) {
+               ++g0;
+               gf += 1.0f;
+               e1 = e2;
+               e2 = fa(fm(gf + 2.0f, dk), im);
+            }
+         }
          float p2 = 0.0f, p1 = 0.0f;
          float cur[4], nxt[4];
          load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
@@ -518,7 +559,7 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
          } else {
             nxt[0] = nxt[1] = nxt[2] = nxt[3] = 0.0f;
          }
-         float face = h4_face(p2, p1, cur[0], cur[1]);
+         float face = h4_face_mode<!EXACT>(p2, p1, cur[0], cur[1]);
          for (int kb = col_s; kb <= col_e; ++kb) {
             float nn[4];
             if (kb + 2 <= col_e) {
@@ -529,12 +570,49 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
             const float w[8] = {p2, p1, cur[0], cur[1], cur[2], cur[3], nxt[0], nxt[1]};
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
-               const float fr = h4_face(w[g + 1], w[g + 2], w[g + 3], w[g + 4]);
+               const float fr = h4_face_mode<!EXACT>(w[g + 1], w[g + 2], w[g + 3], w[g + 4]);
                float a0, a1, a2;
                ppm_coeff(w[g + 1], w[g + 2], w[g + 3], face, fr, threshold, scale, a0, a1, a2);
                face = fr;
                const float v_l = v_r;
                v_r = fa(v_r, dv);
+               if (fused) {
+                  // first target of this source cell: advance past edges <= v_l
+                  // (at most two, as dk > 0.55 dv)
+#pragma unroll
+                  for (int q = 0; q < 2; ++q) {
+                     if (e1 <= v_l) {
+                        ++g0;
+                        gf += 1.0f;
+                        e1 = e2;
+                        e2 = fa(fm(gf + 2.0f, dk), im);
+                     }
+                  }
+                  const float u1 = (e1 >= v_r) ? 1.0f : (e1 - v_l) * inv_dv;
+                  const float u2 = (e2 >= v_r) ? 1.0f : (e2 - v_l) * inv_dv;
+                  const float De = ppm_integral(1.0f, a0, a1, a2);
+                  const float D1 = ppm_integral(u1, a0, a1, a2);
+                  const float D2 = ppm_integral(u2, a0, a1, a2);
+                  const int win_lo = next_flush * WID, win_hi = (next_flush + RING_BLOCKS) * WID - 1;
+                  const int t0 = clampi(g0, gk_lo_col, gk_hi_col);
+                  const int t1 = clampi(g0 + 1, gk_lo_col, gk_hi_col);
+                  const int t2 = clampi(g0 + 2, gk_lo_col, gk_hi_col);
+                  const bool use1 = u1 < 1.0f, use2 = u2 < 1.0f;
+                  range_err |= (t0 < win_lo) | (t0 > win_hi) | (use1 & (t1 > win_hi)) | (use2 & (t2 > win_hi));
+                  if (!range_err) {
+                     float* r0 = &ring[(t0 & (RING_CELLS - 1)) * 16 + lane];
+                     *r0 += D1;
+                     if (use1) {
+                        float* r1 = &ring[(t1 & (RING_CELLS - 1)) * 16 + lane];
+                        *r1 += D2 - D1;
+                     }
+                     if (use2) {
+                        float* r2 = &ring[(t2 & (RING_CELLS - 1)) * 16 + lane];
+                        *r2 += De - D2;
+                     }
+                  }
+                  continue;
+               }
                const int gk_l = gk_r;
                gk_r = __float2int_rz(fd(fs(v_r, im), dk));
                int min_gk = __shfl_sync(hmask, gk_l, min_lane, 16);
@@ -562,7 +640,7 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
             // targets below the next source cell's lower bound are complete
             int lb = ncf * WID;
             if (kb < col_e) {
-               int nl = __shfl_sync(hmask, gk_r, min_lane, 16);
+               int nl = fused ? __reduce_min_sync(hmask, g0) : __shfl_sync(hmask, gk_r, min_lane, 16);
                nl = (nl > gk_lo_col) ? nl : gk_lo_col;
                lb = (nl < lb) ? nl : lb;
             }
@@ -582,7 +660,7 @@ __global__ void __launch_bounds__(REMAP_THREADS) remap_kernel(
          cl = ncl;
       }
       flush_until(1 << 20);
-      if (range_err && lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
+      if (__any_sync(hmask, range_err) && lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
    }
 }
 
@@ -616,16 +694,21 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
-                         uint8_t* content_out, double content_threshold, int grid, cudaStream_t stream) {
-   if (dim == 0)
-      remap_kernel<0><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
-                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
-   else if (dim == 1)
-      remap_kernel<1><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
-                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
-   else
-      remap_kernel<2><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,
-                                                          sweep_cells, status, mesh, wall_margin, set_capacity, content_out, content_threshold);
+                         uint8_t* content_out, double content_threshold, bool exact, int grid, cudaStream_t stream) {
+#define VLGPU_REMAP(D, E)                                                                                     \
+   remap_kernel<D, E><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids, \
+                                                          sweep_cells, status, mesh, wall_margin, set_capacity, \
+                                                          content_out, content_threshold)
+   if (exact) {
+      if (dim == 0) VLGPU_REMAP(0, true);
+      else if (dim == 1) VLGPU_REMAP(1, true);
+      else VLGPU_REMAP(2, true);
+   } else {
+      if (dim == 0) VLGPU_REMAP(0, false);
+      else if (dim == 1) VLGPU_REMAP(1, false);
+      else VLGPU_REMAP(2, false);
+   }
+#undef VLGPU_REMAP
    return cudaGetLastError();
 }
 
@@ -640,7 +723,7 @@ cudaError_t launch_rebase_work(SweepCounters* counters, cudaStream_t stream) {
 
 int remap_blocks_per_sm() {
    int n = 0;
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2>, REMAP_THREADS, 0);
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2, false>, REMAP_THREADS, 0);
    return n > 0 ? n : 1;
 }
 

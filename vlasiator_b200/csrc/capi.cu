@@ -25,7 +25,8 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
-                         uint8_t* content_out, double content_threshold, int grid, cudaStream_t stream);
+                         uint8_t* content_out, double content_threshold, bool exact, int grid,
+                         cudaStream_t stream);
 int remap_blocks_per_sm();
 struct CellAccelInputs {
    double B[3];
@@ -64,6 +65,7 @@ struct vlgpu_batch {
    cudaStream_t stream = nullptr;
    int sm_count = 0;
    int remap_grid = 0;
+   bool exact = false;  // remap arithmetic: false = fused, true = the reference's operation order
    double vmin_d[3], bs_d[3], dv_d[3];
    // data pools and the lists written by sweeps into them
    uint32_t* gids[2] = {nullptr, nullptr};
@@ -186,7 +188,8 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
       const bool prof = b->profiling && b->prof_used + 2 <= b->prof_events.size();
       if (prof) VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used], b->stream));
       VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
-                            sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->remap_grid, b->stream));
+                            sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->remap_grid,
+                            b->stream));
       if (prof) {
          VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used + 1], b->stream));
          b->prof_used += 2;
@@ -202,7 +205,8 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
                                    cap, cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm, c, c + 1,
                                    first_of_step ? 1 : 0, b->stream));
          VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
-                               sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->sm_count, b->stream));
+                               sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->sm_count,
+                               b->stream));
          b->launches += 3;
          b->remap_launches += 1;
       }
@@ -573,7 +577,10 @@ int vlgpu_batch_rho_loss(vlgpu_batch* b, double* out) {
 int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16) {
    if (!b || !out16) return VLGPU_EINVAL;
    VL_CHECK(cudaSetDevice(b->device));
-   int st = moments_device(b, compute_second != 0);
+   // the second-moments pass takes its reference velocity from the record,
+   // so the bulk velocity of the current VDF is computed first
+   int st = moments_device(b, false);
+   if (st == VLGPU_OK && compute_second) st = moments_device(b, true);
    if (st != VLGPU_OK) return st;
    VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
                             b->stream));
@@ -638,6 +645,12 @@ int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out) {
    BatchStats st{};
    VL_CHECK(cudaMemcpy(&st, b->stats, sizeof(st), cudaMemcpyDeviceToHost));
    out[0] = st.step_blocks;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_set_exact(vlgpu_batch* b, int exact) {
+   if (!b) return VLGPU_EINVAL;
+   b->exact = exact != 0;
    return VLGPU_OK;
 }
 

@@ -1,13 +1,15 @@
 // Velocity moments (FP64, Kahan-compensated) and the per-cell FP64
 // acceleration geometry, for sm_100a.
 //
-// moments_kernel: one CTA per cell.  Each thread owns one of the 64 cells
-// of a block (so its velocity offset inside the block is fixed) and walks
-// the cell's blocks with a stride; its partial sums are Kahan-compensated
-// doubles, merged across the CTA with error-free (TwoSum) additions.  The
-// sums are those of blockVelocityFirstMoments / blockVelocitySecondMoments
-// (vlasovsolver/arch_moments.h:83-155) and the per-cell bookkeeping of
-// calculateMoments_V (vlasovsolver/arch_moments.cpp:342-499).
+// moments_kernel: one CTA per cell, one pass over the cell's data.  Sixteen
+// threads share a velocity block, each reading one x-row of four cells as a
+// float4, with several blocks in flight per thread group; per-thread partial
+// sums are Kahan-compensated doubles, merged across the CTA with error-free
+// (TwoSum) additions.  The sums are those of blockVelocityFirstMoments /
+// blockVelocitySecondMoments (vlasovsolver/arch_moments.h:83-155) and the
+// per-cell bookkeeping of calculateMoments_V
+// (vlasovsolver/arch_moments.cpp:342-499); the pressure tensor comes from
+// velocities taken relative to the previous bulk velocity (see the kernel).
 //
 // geometry_kernel: one thread per cell builds the gyration transform and the
 // three intersection sets in FP64 (geometry.cuh) and converts them into the
@@ -60,6 +62,9 @@ __device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, doubl
 }
 
 constexpr int MOM_THREADS = 256;
+constexpr int MOM_GROUPS = MOM_THREADS / 16;  // 16 threads per velocity block
+constexpr int MOM_UNROLL = 4;                 // blocks in flight per thread group
+constexpr int MOM_MAXSUMS = 10;
 
 template <int N>
 __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* sh_hi, double* sh_lo) {
@@ -91,92 +96,117 @@ __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* s
    __syncthreads();
 }
 
+// One CTA per cell; 16 threads per velocity block, each owning one x-row of
+// four cells (a float4: i = 0..3 at j = sub & 3, k = sub >> 2), and every
+// thread group keeps MOM_UNROLL blocks in flight.  With SECOND, velocities
+// are taken relative to a reference velocity U (the cell's bulk velocity in
+// its moment record, written by the first-moments pass that precedes every
+// second-moments pass), so one pass over the data gives both the first
+// moments and the central second moments:
+//   S0 = sum f, S_a = sum f u_a, S_ab = sum f u_a u_b   (u = v - U)
+//   n V_a = (S_a + U_a S0) dv^3,  P_ab = m dv^3 (S_ab - S_a S_b / S0).
+// With U close to V the correction term is small, so nothing cancels; the
+// result equals the reference's two-pass sums (first V, then f (v-V)(v-V))
+// up to FP64 rounding.  Without SECOND, U = 0, so the first moments depend
+// on the data alone.
+template <bool SECOND>
 __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
-   const CellSlot* __restrict__ slots, double* __restrict__ moments, MeshDev mesh, double vmin0, double vmin1, double vmin2, double bs0, double bs1,
-   double bs2, double dv0, double dv1, double dv2, double mass, double charge, int second) {
-   __shared__ double sh_hi[(MOM_THREADS / 32) * 6];
-   __shared__ double sh_lo[(MOM_THREADS / 32) * 6];
-   __shared__ double s_V[3];
+   const CellSlot* __restrict__ slots, double* __restrict__ moments, MeshDev mesh, double vmin0, double vmin1,
+   double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
+   double charge) {
+   constexpr int NS = SECOND ? 10 : 4;
+   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
    const uint32_t cell = blockIdx.x;
    const CellSlot s = slots[cell];
    double* out = moments + (size_t)cell * MOM_COUNT;
-   const int ci = threadIdx.x & 63;
-   const int i = ci & 3, j = (ci >> 2) & 3, k = ci >> 4;
-   const double DV3 = dv0 * dv1 * dv2;
-   const double HALF = 0.5;
-   Kahan acc[5];
-   for (uint32_t b = threadIdx.x >> 6; b < s.count; b += MOM_THREADS / 64) {
-      const uint32_t gid = gids[s.off + b];
-      const uint32_t bi = gid % mesh.len[0], bj = (gid / mesh.len[0]) % mesh.len[1];
-      const uint32_t bk = gid / (mesh.len[0] * mesh.len[1]);
-      const double VX = (vmin0 + bi * bs0) + (i + HALF) * dv0;
-      const double VY = (vmin1 + bj * bs1) + (j + HALF) * dv1;
-      const double VZ = (vmin2 + bk * bs2) + (k + HALF) * dv2;
-      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-      if (idx == 0xffffffffu) continue;  // an added block holds zeros
-      const double f = (double)data[(size_t)idx * WID3 + ci];
-      acc[0].add(f * DV3);
-      acc[1].add(f * VX * DV3);
-      acc[2].add(f * VY * DV3);
-      acc[3].add(f * VZ * DV3);
-      acc[4].add(f);
+   const double U0 = SECOND ? out[MOM_VX] : 0.0, U1 = SECOND ? out[MOM_VY] : 0.0, U2 = SECOND ? out[MOM_VZ] : 0.0;
+   const int sub = threadIdx.x & 15, grp = threadIdx.x >> 4;
+   const int j = sub & 3, k = sub >> 2;
+   const double cy = (j + 0.5) * dv1 - U1, cz = (k + 0.5) * dv2 - U2;
+   const double cx0 = 0.5 * dv0 - U0, cx1 = 1.5 * dv0 - U0, cx2 = 2.5 * dv0 - U0, cx3 = 3.5 * dv0 - U0;
+   const uint32_t L0 = mesh.len[0], L1 = mesh.len[1];
+   Kahan acc[NS];
+   for (uint32_t b0 = grp; b0 < s.count; b0 += MOM_GROUPS * MOM_UNROLL) {
+      uint32_t g[MOM_UNROLL], idx[MOM_UNROLL];
+#pragma unroll
+      for (int u = 0; u < MOM_UNROLL; ++u) {
+         const uint32_t b = b0 + u * MOM_GROUPS;
+         g[u] = (b < s.count) ? __ldg(gids + s.off + b) : 0u;
+         idx[u] = (b < s.count) ? (src_index ? __ldg(src_index + s.off + b) : s.off + b) : 0xffffffffu;
+      }
+      float4 f4[MOM_UNROLL];
+#pragma unroll
+      for (int u = 0; u < MOM_UNROLL; ++u) {
+         f4[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+         if (idx[u] != 0xffffffffu)  // an added block holds zeros
+            f4[u] = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx[u] * WID3) + sub);
+      }
+#pragma unroll
+      for (int u = 0; u < MOM_UNROLL; ++u) {
+         const uint32_t bi = g[u] % L0, bj = (g[u] / L0) % L1, bk = g[u] / (L0 * L1);
+         const double bx = vmin0 + bi * bs0;
+         const double uy = (vmin1 + bj * bs1) + cy;
+         const double uz = (vmin2 + bk * bs2) + cz;
+         const double x0 = bx + cx0, x1 = bx + cx1, x2 = bx + cx2, x3 = bx + cx3;
+         const double f0 = f4[u].x, f1 = f4[u].y, f2 = f4[u].z, f3 = f4[u].w;
+         const double sf = (f0 + f1) + (f2 + f3);
+         const double fx0 = f0 * x0, fx1 = f1 * x1, fx2 = f2 * x2, fx3 = f3 * x3;
+         const double sfx = (fx0 + fx1) + (fx2 + fx3);
+         acc[0].add(sf);
+         acc[1].add(sfx);
+         acc[2].add(sf * uy);
+         acc[3].add(sf * uz);
+         if constexpr (SECOND) {
+            acc[4].add((fx0 * x0 + fx1 * x1) + (fx2 * x2 + fx3 * x3));
+            acc[5].add(sf * uy * uy);
+            acc[6].add(sf * uz * uz);
+            acc[7].add(sf * uy * uz);
+            acc[8].add(sfx * uz);
+            acc[9].add(sfx * uy);
+         }
+      }
    }
-   double hi[6], lo[6];
-   for (int q = 0; q < 5; ++q) {
+   double hi[NS], lo[NS];
+#pragma unroll
+   for (int q = 0; q < NS; ++q) {
       hi[q] = acc[q].s;
       lo[q] = -acc[q].c;
    }
-   hi[5] = lo[5] = 0.0;
-   cta_reduce<5>(hi, lo, sh_hi, sh_lo);
-   if (threadIdx.x == 0) {
-      const double a0 = hi[0] + lo[0], a1 = hi[1] + lo[1], a2 = hi[2] + lo[2], a3 = hi[3] + lo[3];
-      out[MOM_N] = a0;
-      out[MOM_NVX] = a1;
-      out[MOM_NVY] = a2;
-      out[MOM_NVZ] = a3;
-      const double rhom = a0 * mass;
-      out[MOM_RHOM] = rhom;
-      const double vx = (rhom != 0.0) ? (a1 * mass) / rhom : 0.0;
-      const double vy = (rhom != 0.0) ? (a2 * mass) / rhom : 0.0;
-      const double vz = (rhom != 0.0) ? (a3 * mass) / rhom : 0.0;
-      out[MOM_VX] = vx;
-      out[MOM_VY] = vy;
-      out[MOM_VZ] = vz;
-      out[MOM_RHOQ] = a0 * charge;
-      out[MOM_MASS] = hi[4] + lo[4];
-      s_V[0] = vx;
-      s_V[1] = vy;
-      s_V[2] = vz;
+   cta_reduce<NS>(hi, lo, sh_hi, sh_lo);
+   if (threadIdx.x != 0) return;
+   double S[NS];
+#pragma unroll
+   for (int q = 0; q < NS; ++q) S[q] = hi[q] + lo[q];
+   const double DV3 = dv0 * dv1 * dv2;
+   const double a0 = S[0] * DV3;
+   const double a1 = (S[1] + U0 * S[0]) * DV3, a2 = (S[2] + U1 * S[0]) * DV3, a3 = (S[3] + U2 * S[0]) * DV3;
+   out[MOM_N] = a0;
+   out[MOM_NVX] = a1;
+   out[MOM_NVY] = a2;
+   out[MOM_NVZ] = a3;
+   const double rhom = a0 * mass;
+   out[MOM_RHOM] = rhom;
+   out[MOM_VX] = (rhom != 0.0) ? (a1 * mass) / rhom : 0.0;
+   out[MOM_VY] = (rhom != 0.0) ? (a2 * mass) / rhom : 0.0;
+   out[MOM_VZ] = (rhom != 0.0) ? (a3 * mass) / rhom : 0.0;
+   out[MOM_RHOQ] = a0 * charge;
+   out[MOM_MASS] = S[0];
+   double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+   if constexpr (SECOND) {
+      if (S[0] != 0.0) {
+         const double m1 = S[1] / S[0], m2 = S[2] / S[0], m3 = S[3] / S[0];
+         const double pre = mass * DV3;
+         P[0] = pre * (S[4] - S[1] * m1);
+         P[1] = pre * (S[5] - S[2] * m2);
+         P[2] = pre * (S[6] - S[3] * m3);
+         P[3] = pre * (S[7] - S[2] * m3);
+         P[4] = pre * (S[8] - S[1] * m3);
+         P[5] = pre * (S[9] - S[1] * m2);
+      }
    }
-   if (!second) return;
-   __syncthreads();
-   const double aVX = s_V[0], aVY = s_V[1], aVZ = s_V[2];
-   Kahan p[6];
-   for (uint32_t b = threadIdx.x >> 6; b < s.count; b += MOM_THREADS / 64) {
-      const uint32_t gid = gids[s.off + b];
-      const uint32_t bi = gid % mesh.len[0], bj = (gid / mesh.len[0]) % mesh.len[1];
-      const uint32_t bk = gid / (mesh.len[0] * mesh.len[1]);
-      const double VX = (vmin0 + bi * bs0) + (i + HALF) * dv0;
-      const double VY = (vmin1 + bj * bs1) + (j + HALF) * dv1;
-      const double VZ = (vmin2 + bk * bs2) + (k + HALF) * dv2;
-      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-      if (idx == 0xffffffffu) continue;
-      const double f = (double)data[(size_t)idx * WID3 + ci];
-      p[0].add(f * (VX - aVX) * (VX - aVX) * DV3);
-      p[1].add(f * (VY - aVY) * (VY - aVY) * DV3);
-      p[2].add(f * (VZ - aVZ) * (VZ - aVZ) * DV3);
-      p[3].add(f * (VY - aVY) * (VZ - aVZ) * DV3);
-      p[4].add(f * (VX - aVX) * (VZ - aVZ) * DV3);
-      p[5].add(f * (VX - aVX) * (VY - aVY) * DV3);
-   }
-   for (int q = 0; q < 6; ++q) {
-      hi[q] = p[q].s;
-      lo[q] = -p[q].c;
-   }
-   cta_reduce<6>(hi, lo, sh_hi, sh_lo);
-   if (threadIdx.x == 0)
-      for (int q = 0; q < 6; ++q) out[MOM_P11 + q] = mass * (hi[q] + lo[q]);
+   for (int q = 0; q < 6; ++q) out[MOM_P11 + q] = P[q];
 }
 
 // Per-cell acceleration inputs on the device.
@@ -238,9 +268,14 @@ cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, cons
                            const MeshDev& mesh, const double vmin[3], const double bs[3], const double dv[3],
                            double mass, double charge, bool second, uint32_t n_cells, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
-   moments_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, mesh, vmin[0], vmin[1], vmin[2],
-                                                       bs[0], bs[1], bs[2], dv[0], dv[1], dv[2], mass, charge,
-                                                       second ? 1 : 0);
+   if (second)
+      moments_kernel<true><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, mesh, vmin[0],
+                                                               vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0], dv[1],
+                                                               dv[2], mass, charge);
+   else
+      moments_kernel<false><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, mesh, vmin[0],
+                                                                vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0], dv[1],
+                                                                dv[2], mass, charge);
    return cudaGetLastError();
 }
 

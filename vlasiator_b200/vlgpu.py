@@ -82,6 +82,7 @@ SIGNATURES = {
     "vlgpu_batch_stats2": (ctypes.c_int, [_vp, _u64p]),
     "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
+    "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
                                             _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
                                             _u32p, _vp]),
@@ -127,7 +128,7 @@ class Batch:
     """A device-resident batch of spatial cells (one population)."""
 
     def __init__(self, mesh: VelocityMesh, n_cells: int, capacity: int, params: CParamsT | None = None,
-                 device: int = 0):
+                 device: int = 0, exact: bool = False):
         self.lib = load()
         self.mesh = mesh
         self.n_cells = int(n_cells)
@@ -140,6 +141,12 @@ class Batch:
         _check(self.lib.vlgpu_batch_create(ctypes.byref(m), ctypes.byref(self.params), self.n_cells, self.capacity,
                                            device, ctypes.byref(h)), "vlgpu_batch_create")
         self.h = h
+        self.set_exact(exact)
+
+    def set_exact(self, exact: bool):
+        """exact=True: bit-identical to the reference's map_1d; False: fused remap (1e-5 of peak)."""
+        _check(self.lib.vlgpu_batch_set_exact(self.h, int(bool(exact))), "vlgpu_batch_set_exact")
+        self.exact = bool(exact)
 
     def close(self):
         if getattr(self, "h", None):
