@@ -101,6 +101,38 @@ __device__ __forceinline__ void ppm_coeff(float vm1, float v0, float vp1, float 
    a2 = fs(fa(fl, fr), fm(2.0f, v0));
 }
 
+// The same coefficients in plain single precision (fused mode): the superbee
+// slope as sign(a) * max(min(|a|, 2|b|), min(2|a|, |b|)) when a and b share a
+// sign (equal to maxmod(minmod(a, 2b), minmod(2a, b))), on unscaled values
+// with sign tests instead of products, and contractible arithmetic.
+__device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, float fl, float fr, float& a0,
+                                                float& a1, float& a2) {
+   const float a = vp1 - v0, b = v0 - vm1;
+   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const float aa = fabsf(a), ab = fabsf(b);
+   const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
+   if (sl == 0.0f) {
+      fl = v0;
+      fr = v0;
+   }
+   const float hs = copysignf(0.5f * sl, a);
+   if ((vm1 - fl) * (fl - v0) < 0.0f) fl = v0 - hs;
+   if ((vp1 - fr) * (fr - v0) < 0.0f) fr = v0 + hs;
+   const float one_sixth = (float)(1.0 / 6.0);
+   const float v3 = 3.0f * v0;
+   {
+      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
+      if (d * e > d * d * one_sixth) fl = v3 - 2.0f * fr;
+   }
+   {
+      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
+      if (-d * d * one_sixth > d * e) fr = v3 - 2.0f * fl;
+   }
+   a0 = fl;
+   a1 = v3 - 2.0f * fl - fr;
+   a2 = fl + fr - 2.0f * v0;
+}
+
 // ---------------------------------------------------------------------------
 // 96-bit mask helpers
 // ---------------------------------------------------------------------------
@@ -539,10 +571,20 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
          }
          const int gk_lo_col = cf * WID, gk_hi_col = (cl + 1) * WID - 1;
          // fused mode: g0 = the lane's first target (edge(g0+1) > v), e1/e2 =
-         // edge(g0+1)/edge(g0+2), gf = g0 as a float
+         // edge(g0+1)/edge(g0+2), gf = g0 as a float; acc0..acc2 hold the
+         // mass of targets g0..g0+2, which pass into the ring as g0 advances
          int g0 = gk_r - 2;
          float gf = (float)g0;
          float e1 = fa(fm(gf + 1.0f, dk), im), e2 = fa(fm(gf + 2.0f, dk), im);
+         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+         auto evict = [&](float acc, int g) {
+            if (acc != 0.0f) {
+               const int t = clampi(g, gk_lo_col, gk_hi_col);
+               range_err |= (t < next_flush * WID) | (t >= (next_flush + RING_BLOCKS) * WID);
+               float* r = &ring[(t & (RING_CELLS - 1)) * 16 + lane];
+               *r += acc;
+            }
+         };
          if (fused) {
             for (int q = 0; q < 6 && e1 <= v_r; ++q) {
                ++g0;
@@ -572,45 +614,40 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
             for (int g = 0; g < 4; ++g) {
                const float fr = h4_face_mode<!EXACT>(w[g + 1], w[g + 2], w[g + 3], w[g + 4]);
                float a0, a1, a2;
-               ppm_coeff(w[g + 1], w[g + 2], w[g + 3], face, fr, threshold, scale, a0, a1, a2);
+               if constexpr (EXACT)
+                  ppm_coeff(w[g + 1], w[g + 2], w[g + 3], face, fr, threshold, scale, a0, a1, a2);
+               else
+                  ppm_coeff_fused(w[g + 1], w[g + 2], w[g + 3], face, fr, a0, a1, a2);
                face = fr;
                const float v_l = v_r;
                v_r = fa(v_r, dv);
                if (fused) {
                   // first target of this source cell: advance past edges <= v_l
-                  // (at most two, as dk > 0.55 dv)
+                  // (at most two, as dk > 0.55 dv), handing finished targets
+                  // to the ring
 #pragma unroll
                   for (int q = 0; q < 2; ++q) {
                      if (e1 <= v_l) {
+                        evict(acc0, g0);
+                        acc0 = acc1;
+                        acc1 = acc2;
+                        acc2 = 0.0f;
                         ++g0;
                         gf += 1.0f;
                         e1 = e2;
                         e2 = fa(fm(gf + 2.0f, dk), im);
                      }
                   }
+                  // integrals up to the two edges inside the source cell; if
+                  // e1 lies beyond v_r then so does e2 and D1 = D2 = De
                   const float u1 = (e1 >= v_r) ? 1.0f : (e1 - v_l) * inv_dv;
                   const float u2 = (e2 >= v_r) ? 1.0f : (e2 - v_l) * inv_dv;
                   const float De = ppm_integral(1.0f, a0, a1, a2);
                   const float D1 = ppm_integral(u1, a0, a1, a2);
                   const float D2 = ppm_integral(u2, a0, a1, a2);
-                  const int win_lo = next_flush * WID, win_hi = (next_flush + RING_BLOCKS) * WID - 1;
-                  const int t0 = clampi(g0, gk_lo_col, gk_hi_col);
-                  const int t1 = clampi(g0 + 1, gk_lo_col, gk_hi_col);
-                  const int t2 = clampi(g0 + 2, gk_lo_col, gk_hi_col);
-                  const bool use1 = u1 < 1.0f, use2 = u2 < 1.0f;
-                  range_err |= (t0 < win_lo) | (t0 > win_hi) | (use1 & (t1 > win_hi)) | (use2 & (t2 > win_hi));
-                  if (!range_err) {
-                     float* r0 = &ring[(t0 & (RING_CELLS - 1)) * 16 + lane];
-                     *r0 += D1;
-                     if (use1) {
-                        float* r1 = &ring[(t1 & (RING_CELLS - 1)) * 16 + lane];
-                        *r1 += D2 - D1;
-                     }
-                     if (use2) {
-                        float* r2 = &ring[(t2 & (RING_CELLS - 1)) * 16 + lane];
-                        *r2 += De - D2;
-                     }
-                  }
+                  acc0 += D1;
+                  acc1 += D2 - D1;
+                  acc2 += De - D2;
                   continue;
                }
                const int gk_l = gk_r;
@@ -636,6 +673,12 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
                      }
                   }
                }
+            }
+            if (fused && kb == col_e) {
+               // column done: its last targets go to the ring before the flush
+               evict(acc0, g0);
+               evict(acc1, g0 + 1);
+               evict(acc2, g0 + 2);
             }
             // targets below the next source cell's lower bound are complete
             int lb = ncf * WID;
