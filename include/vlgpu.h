@@ -176,6 +176,22 @@ int vlgpu_accelerate_device(vlgpu_batch* b, uint32_t map_order);
    plain per-cell path, kept as the drop-in baseline of the batched one. */
 int vlgpu_accelerate_per_cell(vlgpu_batch* b, uint32_t map_order);
 
+/* ---- spatial translation ------------------------------------------------ */
+
+/* Declares the batch's cells to be a uniform periodic spatial grid of
+   dims[0] x dims[1] x dims[2] cells (x fastest: cell = x + dims[0]*(y +
+   dims[1]*z); dims[0]*dims[1]*dims[2] == n_cells, each dims[d] <= 128) with
+   cell sizes dx[3] (m), as the reference's DX/DY/DZ cell parameters.  Adds
+   translation work arrays sized from the block capacity. */
+int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx[3]);
+
+/* One translation sweep along `dimension` of every cell of the grid over dt
+   seconds: trans_map_1d_amr (vlasovsolver/cpu_trans_map_amr.cpp:214-443,
+   propagatePencil :37-150) for pencils through a uniform periodic grid.
+   Block sets do not change; mass flowing into a cell that lacks the block is
+   dropped, as in the reference. */
+int vlgpu_translate(vlgpu_batch* b, uint32_t dimension, double dt);
+
 /* Block adjustment of every cell (SpatialCell::adjust_velocity_blocks,
    spatial_cells/spatial_cell_cpu.cpp:179-273, no spatial neighbours):
    keeps the blocks with content and their +-blockAddWidthV velocity

@@ -49,6 +49,23 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           uint32_t n_cells, cudaStream_t stream);
 cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
                                cudaStream_t stream);
+struct TransCounters {
+   uint32_t n_items;
+   uint32_t work;
+   uint32_t overflow;
+   uint32_t pad;
+};
+constexpr uint32_t TR_MAX_N = 128;
+cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int dim, uint32_t nx, uint32_t ny,
+                                uint32_t nz, const MeshDev& mesh, uint32_t* item_gid, uint32_t* item_pencil,
+                                uint32_t* rows, uint32_t item_cap, uint64_t row_cap, TransCounters* tc,
+                                uint32_t* status, cudaStream_t stream);
+cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, const uint32_t* item_pencil,
+                               const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
+                               const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
+                               float dz, float threshold, int grid, cudaStream_t stream);
+int trans_blocks_per_sm(uint32_t N);
+uint32_t union_words(const MeshDev& mesh);
 constexpr int MOM_COUNT = 16;
 constexpr double MU_0 = 1.25663706e-6;  // physicalconstants::MU_0 (common.h:561)
 }  // namespace vlgpu
@@ -95,6 +112,15 @@ struct vlgpu_batch {
    uint32_t* status = nullptr;
    SweepCounters* counters = nullptr;
    BatchStats* stats = nullptr;
+   // spatial grid (uniform, periodic, cells x fastest) and translation work arrays
+   bool has_grid = false;
+   uint32_t grid_dims[3] = {0, 0, 0};
+   double grid_dx[3] = {0.0, 0.0, 0.0};
+   uint32_t* item_gid = nullptr;
+   uint32_t* item_pencil = nullptr;
+   uint32_t* trans_rows = nullptr;
+   uint64_t row_cap = 0;
+   TransCounters* tcounters = nullptr;
    // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;
    CellAccelInputs* h_accel = nullptr;
@@ -144,6 +170,10 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->status);
    cudaFree(b->counters);
    cudaFree(b->stats);
+   cudaFree(b->item_gid);
+   cudaFree(b->item_pencil);
+   cudaFree(b->trans_rows);
+   cudaFree(b->tcounters);
    for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
    cudaFreeHost(b->h_sweep);
    cudaFreeHost(b->h_accel);
@@ -293,6 +323,27 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
    st = adjust_device(b);
    if (st != VLGPU_OK) return st;
    return moments_device(b, true);
+}
+
+// One translation sweep of the whole grid along `dim` (trans_map_1d_amr):
+// out of place into the other pool, same block lists.
+int translate_device(vlgpu_batch* b, uint32_t dim, double dt) {
+   const int d = 1 - b->cur;
+   const uint32_t N = b->grid_dims[dim];
+   VL_CHECK(cudaMemsetAsync(b->tcounters, 0, sizeof(TransCounters), b->stream));
+   VL_CHECK(launch_pencil_union(b->st_gids, b->st_slots, (int)dim, b->grid_dims[0], b->grid_dims[1],
+                                b->grid_dims[2], b->mdev, b->item_gid, b->item_pencil, b->trans_rows,
+                                (uint32_t)b->capacity, b->row_cap, b->tcounters, b->status, b->stream));
+   const int grid = b->sm_count * trans_blocks_per_sm(N);
+   VL_CHECK(launch_trans_remap((int)dim, N, b->item_gid, b->item_pencil, b->trans_rows, b->tcounters,
+                               (uint32_t)b->capacity, b->st_src, b->data[b->cur], b->data[d], b->gids[d], b->mdev,
+                               (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, grid, b->stream));
+   VL_CHECK(cudaMemcpyAsync(b->slots[d], b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToDevice,
+                            b->stream));
+   b->launches += 2;
+   set_direct_state(b, d);
+   b->content_valid = false;
+   return VLGPU_OK;
 }
 
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
@@ -648,6 +699,37 @@ int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out) {
    return VLGPU_OK;
 }
 
+int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx[3]) {
+   if (!b || !dims || !dx) return VLGPU_EINVAL;
+   if ((uint64_t)dims[0] * dims[1] * dims[2] != b->n_cells) return VLGPU_EINVAL;
+   for (int d = 0; d < 3; ++d)
+      if (dims[d] == 0 || dims[d] > TR_MAX_N || !(dx[d] > 0.0)) return VLGPU_EINVAL;
+   if (union_words(b->mdev) > 12288) return VLGPU_EINVAL;  // union bitmap and prefix fit in 96 KB
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   if (!b->item_gid) {
+      const uint64_t cap = b->capacity;
+      b->row_cap = 4 * cap;
+      VL_CHECK(cudaMalloc(&b->item_gid, sizeof(uint32_t) * cap));
+      VL_CHECK(cudaMalloc(&b->item_pencil, sizeof(uint32_t) * cap));
+      VL_CHECK(cudaMalloc(&b->trans_rows, sizeof(uint32_t) * b->row_cap));
+      VL_CHECK(cudaMalloc(&b->tcounters, sizeof(TransCounters)));
+      VL_CHECK(cudaMemset(b->tcounters, 0, sizeof(TransCounters)));
+   }
+   for (int d = 0; d < 3; ++d) {
+      b->grid_dims[d] = dims[d];
+      b->grid_dx[d] = dx[d];
+   }
+   b->has_grid = true;
+   return VLGPU_OK;
+}
+
+int vlgpu_translate(vlgpu_batch* b, uint32_t dimension, double dt) {
+   if (!b || dimension > 2 || !b->has_grid) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return translate_device(b, dimension, dt);
+}
+
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact) {
    if (!b) return VLGPU_EINVAL;
    b->exact = exact != 0;
@@ -661,6 +743,11 @@ int vlgpu_batch_sync(vlgpu_batch* b) {
    SweepCounters c{};
    VL_CHECK(cudaMemcpy(&c, b->counters, sizeof(c), cudaMemcpyDeviceToHost));
    if (c.overflow) return VLGPU_ENOMEM;
+   if (b->tcounters) {
+      TransCounters t{};
+      VL_CHECK(cudaMemcpy(&t, b->tcounters, sizeof(t), cudaMemcpyDeviceToHost));
+      if (t.overflow) return VLGPU_ENOMEM;
+   }
    return VLGPU_OK;
 }
 

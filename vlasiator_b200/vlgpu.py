@@ -83,6 +83,8 @@ SIGNATURES = {
     "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
     "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "vlgpu_batch_set_grid": (ctypes.c_int, [_vp, _u32p, _dp]),
+    "vlgpu_translate": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_double]),
     "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
                                             _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
                                             _u32p, _vp]),
@@ -264,6 +266,18 @@ class Batch:
     def accelerate_device(self, map_order: int, per_cell: bool = False):
         fn = self.lib.vlgpu_accelerate_per_cell if per_cell else self.lib.vlgpu_accelerate_device
         _check(fn(self.h, map_order), "vlgpu_accelerate_device")
+
+    # ---- spatial translation ----
+    def set_grid(self, dims, dx):
+        """Cells form a uniform periodic grid dims (x fastest) with cell sizes dx (m)."""
+        d = np.ascontiguousarray(dims, np.uint32)
+        h = np.ascontiguousarray(np.broadcast_to(np.asarray(dx, np.float64), (3,)))
+        _check(self.lib.vlgpu_batch_set_grid(self.h, _p(d, ctypes.c_uint32), _p(h, ctypes.c_double)),
+               "vlgpu_batch_set_grid")
+
+    def translate(self, dim: int, dt: float):
+        """One translation sweep (trans_map_1d_amr) along dim over dt seconds."""
+        _check(self.lib.vlgpu_translate(self.h, dim, float(dt)), "vlgpu_translate")
 
     def adjust(self):
         _check(self.lib.vlgpu_adjust_blocks(self.h), "vlgpu_adjust_blocks")
