@@ -192,10 +192,37 @@ int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx
    dropped, as in the reference. */
 int vlgpu_translate(vlgpu_batch* b, uint32_t dimension, double dt);
 
+/* One full Vlasov step of the grid over dt seconds, in the reference's main
+   loop order: translation along z, x, y (calculateSpatialTranslation,
+   vlasovsolver/vlasovmover.cpp:65-381) with the "_R" moments after it
+   (calculateMoments_R, arch_moments.cpp), then one acceleration step with
+   fields[] (one per cell, host) and map_order as vlgpu_accelerate does it,
+   whose block adjustment consults the spatial neighbours (adjustVelocityBlocks
+   with the full neighbour lists, vlasovmover.cpp:564-569).  One subcycle. */
+int vlgpu_vlasov_step(vlgpu_batch* b, const vlgpu_cell_fields* fields, double dt, uint32_t map_order);
+
+/* The same step reusing the fields last passed (no host data; the
+   acceleration uses the per-cell dt last staged). */
+int vlgpu_vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);
+
+/* The "_R" moments computed after the last translation of a Vlasov step, in
+   the layout of vlgpu_batch_moments (16 doubles per cell). */
+int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16);
+
+/* Time-step limits per cell (host arrays of n_cells): r_dt = the r-space
+   limit of reduce_vlasov_dt (vlasovsolver/arch_dt.cpp:34-97) from the cell's
+   current blocks and the grid's cell sizes; v_dt = the v-space limit of
+   updateAccelerationMaxdt (cpu_acc_transform.cpp:41-55), |gyroperiod| *
+   max_rotation_deg / 360 from the fields last passed to vlgpu_accelerate or
+   vlgpu_compute_intersections.  The batch must be a grid. */
+int vlgpu_batch_max_dt(vlgpu_batch* b, double max_rotation_deg, double* r_dt, double* v_dt);
+
 /* Block adjustment of every cell (SpatialCell::adjust_velocity_blocks,
-   spatial_cells/spatial_cell_cpu.cpp:179-273, no spatial neighbours):
-   keeps the blocks with content and their +-blockAddWidthV velocity
-   neighbours, removes the rest, adds missing neighbours with zero data. */
+   spatial_cells/spatial_cell_cpu.cpp:179-273): keeps the blocks with content and their +-blockAddWidthV velocity
+   neighbours and, when the batch is a grid (vlgpu_batch_set_grid), every
+   block with content in one of the cell's 26 nearest spatial neighbours
+   (adjustVelocityBlocks, grid.cpp:775-817); removes the rest, adds missing
+   blocks with zero data. */
 int vlgpu_adjust_blocks(vlgpu_batch* b);
 
 /* Mass removed by block adjustment per cell since the last upload

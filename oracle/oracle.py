@@ -18,6 +18,7 @@ import subprocess
 
 import numpy as np
 
+from vlasiator_b200.grid import grid_neighbors
 from vlasiator_b200.mesh import WID3, CMesh, VelocityMesh
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -66,6 +67,12 @@ class Restatement:
         L.orc_adjust.restype = ctypes.c_int
         L.orc_adjust.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double,
                                  ctypes.c_int, ctypes.c_uint32, _u32p, _u32p, ctypes.POINTER(ct), _dp]
+        L.orc_adjust_with.restype = ctypes.c_int
+        L.orc_adjust_with.argtypes = [ctypes.POINTER(CMesh), ctypes.c_uint32, _u32p, ctypes.POINTER(ct),
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_uint32, _u32p, ctypes.c_uint32, _u32p,
+                                      _u32p, ctypes.POINTER(ct), _dp]
+        L.orc_content_gids.restype = ctypes.c_uint32
+        L.orc_content_gids.argtypes = [ctypes.c_uint32, _u32p, ctypes.POINTER(ct), ctypes.c_double, _u32p]
 
     def map_1d(self, mesh: VelocityMesh, gids, data, isect4, dim: int, min_value: float, wall_margin: int = 1,
                cap: int | None = None):
@@ -110,6 +117,43 @@ class Restatement:
             raise RuntimeError(f"orc_adjust failed with status {rc}")
         return go[: n.value].copy(), do[: n.value].copy(), loss.value
 
+    def content_gids(self, gids, data, min_value):
+        gids = np.ascontiguousarray(gids, dtype=np.uint32)
+        data = np.ascontiguousarray(data, dtype=self.realf).reshape(-1, WID3)
+        out = np.zeros(max(len(gids), 1), np.uint32)
+        k = self.lib.orc_content_gids(len(gids), _ptr(gids, ctypes.c_uint32), _ptr(data, self._ct),
+                                      float(min_value), _ptr(out, ctypes.c_uint32))
+        return out[:k].copy()
+
+    def adjust_grid(self, mesh: VelocityMesh, grid, cells, min_value, add_width=1):
+        """adjustVelocityBlocks (grid.cpp:775-817) over a uniform periodic grid:
+        content lists of every cell first, then each cell adjusted with the
+        content of its 26 nearest neighbours.  cells: [(gids, data)] x fastest.
+        Returns [(gids sorted, data)], loss per cell."""
+        content = [self.content_gids(g, d, min_value) for g, d in cells]
+        nbrs = grid_neighbors(grid)
+        out, losses = [], []
+        cm = CMesh.of(mesh)
+        for c, (g, d) in enumerate(cells):
+            extra = np.unique(np.concatenate([content[n] for n in nbrs[c] if n >= 0] + [np.zeros(0, np.uint32)]))
+            extra = np.ascontiguousarray(extra, np.uint32)
+            g = np.ascontiguousarray(g, np.uint32)
+            d = np.ascontiguousarray(d, self.realf).reshape(-1, WID3)
+            cap = max(30 * len(g) + len(extra) + 64, 1024)
+            go = np.zeros(cap, np.uint32)
+            do = np.zeros((cap, WID3), self.realf)
+            n = ctypes.c_uint32(0)
+            loss = ctypes.c_double(0)
+            rc = self.lib.orc_adjust_with(ctypes.byref(cm), len(g), _ptr(g, ctypes.c_uint32), _ptr(d, self._ct),
+                                          float(min_value), int(add_width), len(extra),
+                                          _ptr(extra, ctypes.c_uint32), cap, ctypes.byref(n),
+                                          _ptr(go, ctypes.c_uint32), _ptr(do, self._ct), ctypes.byref(loss))
+            if rc != 0:
+                raise RuntimeError(f"orc_adjust_with failed with status {rc}")
+            out.append((go[: n.value].copy(), do[: n.value].copy()))
+            losses.append(loss.value)
+        return out, np.array(losses)
+
     def translate(self, mesh: VelocityMesh, grid, offsets, gids, data, dim, dt, dz, min_value=1e-15):
         """One spatial dimension of the translation of a uniform periodic grid (cells x fastest)."""
         g3 = np.ascontiguousarray(grid, np.uint32)
@@ -142,6 +186,38 @@ class Restatement:
         g, d, loss = self.adjust(mesh, g, d, min_value, add_width)
         m1 = self.moments(mesh, g, d, mass, charge, second=True)
         return g, d, isect, loss, m1, wall
+
+    def vlasov_step(self, mesh: VelocityMesh, grid, cells, B, dt, map_order, dx, mass, charge, min_value=1e-15,
+                    add_width=1, hall_min_rhoq=1.60217653e-19, mu0=1.25663706e-6):
+        """One Vlasov step of a uniform periodic grid in the reference's main-loop
+        order: calculateSpatialTranslation (vlasovmover.cpp:65-381: z, x, y, then
+        calculateMoments_R), then calculateAcceleration for one subcycle
+        (vlasovmover.cpp:410-475: moments_V, transform, intersections, three
+        map_1d per cell) and its final adjustVelocityBlocks with the spatial
+        neighbours plus calculateMoments_V (vlasovmover.cpp:564-569).
+        cells: [(gids, data)] x fastest.  Returns (cells sorted by GID, loss per
+        cell, moments_R, moments_V, intersections)."""
+        state = [(np.asarray(g, np.uint32), np.asarray(d, self.realf).reshape(-1, WID3)) for g, d in cells]
+        for dim in (2, 0, 1):
+            offs = np.zeros(len(state) + 1, np.uint64)
+            offs[1:] = np.cumsum([len(g) for g, _ in state])
+            out = self.translate(mesh, grid, offs, np.concatenate([g for g, _ in state]),
+                                 np.concatenate([d for _, d in state]), dim, dt, dx[dim], min_value)
+            state = [(g, out[offs[c]:offs[c + 1]]) for c, (g, _) in enumerate(state)]
+        mom_r = np.stack([self.moments(mesh, g, d, mass, charge, second=True) for g, d in state])
+        swept, isects = [], []
+        for c, (g, d) in enumerate(state):
+            m0 = self.moments(mesh, g, d, mass, charge, second=False)
+            L, t = self.acceleration_transform(B[c], np.zeros(3), m0[8], m0[5:8], np.zeros(3), charge, mass, dt,
+                                               hall_min_rhoq, 0, mu0)
+            isect = self.cell_intersections(L, t, mesh, map_order)
+            for dim in [[0, 1, 2], [1, 2, 0], [2, 0, 1]][map_order]:
+                g, d, _ = self.map_1d(mesh, g, d, isect[4 * dim:4 * dim + 4], dim, min_value)
+            swept.append((g, d))
+            isects.append(isect)
+        adjusted, loss = self.adjust_grid(mesh, grid, swept, min_value, add_width)
+        mom_v = np.stack([self.moments(mesh, g, d, mass, charge, second=True) for g, d in adjusted])
+        return adjusted, loss, mom_r, mom_v, np.stack(isects)
 
     def acceleration_transform(self, B, curl, rhoq, V, egradpe, q, m, dt, hall_min_rhoq, ohm_gradpe, mu0):
         L = np.zeros(9)

@@ -686,14 +686,20 @@ void orc_moments(const orc_mesh* m, uint32_t n, const uint32_t* gids, const real
 /* the mesh; kept blocks keep their data, added ones are zero, the removed   */
 /* mass sum(f)*dv^3 is returned in *loss.  Output sorted by global ID.        */
 /* ------------------------------------------------------------------------- */
-int orc_adjust(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf* data, double min_value,
-               int add_width, uint32_t cap, uint32_t* n_out, uint32_t* gids_out, realf* data_out, double* loss) {
+/* With spatial neighbours: extra[0..n_extra) are the global IDs of the      */
+/* blocks with content in the cell's spatial neighbours                       */
+/* (spatial_cell_cpu.cpp:211-221); they join the kept set as they are.       */
+int orc_adjust_with(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf* data, double min_value,
+                    int add_width, uint32_t n_extra, const uint32_t* extra, uint32_t cap, uint32_t* n_out,
+                    uint32_t* gids_out, realf* data_out, double* loss) {
    const uint32_t L0 = m->len[0], L1 = m->len[1], L2 = m->len[2];
    const size_t nb = (size_t)L0 * L1 * L2;
    int32_t* where = (int32_t*)malloc(sizeof(int32_t) * nb);
    unsigned char* keep = (unsigned char*)calloc(nb, 1);
    if (!where || !keep) { free(where); free(keep); return ORC_ENOMEM; }
    for (size_t q = 0; q < nb; ++q) where[q] = -1;
+   for (uint32_t q = 0; q < n_extra; ++q)
+      if (extra[q] < nb) keep[extra[q]] = 1;
    for (uint32_t b = 0; b < n; ++b) where[gids[b]] = (int32_t)b;
    for (uint32_t b = 0; b < n; ++b) {
       int content = 0;
@@ -734,6 +740,25 @@ int orc_adjust(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf*
    free(where);
    free(keep);
    return status;
+}
+
+int orc_adjust(const orc_mesh* m, uint32_t n, const uint32_t* gids, const realf* data, double min_value,
+               int add_width, uint32_t cap, uint32_t* n_out, uint32_t* gids_out, realf* data_out, double* loss) {
+   return orc_adjust_with(m, n, gids, data, min_value, add_width, 0, NULL, cap, n_out, gids_out, data_out, loss);
+}
+
+/* The global IDs of the blocks with content (compute_block_has_content,      */
+/* spatial_cell_cpu.cpp:290-320); returns their number.                       */
+uint32_t orc_content_gids(uint32_t n, const uint32_t* gids, const realf* data, double min_value, uint32_t* out) {
+   uint32_t k = 0;
+   for (uint32_t b = 0; b < n; ++b) {
+      for (int c = 0; c < WID3; ++c)
+         if ((double)data[(size_t)b * WID3 + c] >= min_value) {
+            out[k++] = gids[b];
+            break;
+         }
+   }
+   return k;
 }
 
 /* ------------------------------------------------------------------------- */

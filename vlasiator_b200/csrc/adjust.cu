@@ -1,10 +1,12 @@
 // Sparse velocity-block adjustment for sm_100a.
 //
 // Semantics of SpatialCell::adjust_velocity_blocks
-// (spatial_cells/spatial_cell_cpu.cpp:179-273) for cells without spatial
-// neighbours: the new block set is H = the blocks with content (any cell >=
-// minValue, compute_block_has_content, spatial_cell_cpu.cpp:290-320) dilated
-// by +-blockAddWidthV in all three velocity directions, clipped to the mesh.
+// (spatial_cells/spatial_cell_cpu.cpp:179-273): the new block set is H = the
+// blocks with content (any cell >= minValue, compute_block_has_content,
+// spatial_cell_cpu.cpp:290-320) dilated by +-blockAddWidthV in all three
+// velocity directions, clipped to the mesh, plus every block that has content
+// in one of the cell's spatial neighbours (the 26 nearest cells of a periodic
+// grid, Neighborhoods::NEAREST of grid.cpp:979-997), when the batch is a grid.
 // Blocks with content always stay, blocks in H keep their data, blocks not
 // in H are removed and their mass sum(f)*dv^3 is added to RHOLOSSADJUST,
 // blocks of H that did not exist are added with zero data.
@@ -77,15 +79,24 @@ __device__ __forceinline__ uint32_t shr96(uint32_t w0, uint32_t w1, uint32_t w2,
    return w2 >> s;
 }
 
+__device__ __forceinline__ bool list_block_content(const uint32_t* __restrict__ src_index,
+                                                   const uint8_t* __restrict__ content,
+                                                   const float* __restrict__ data, uint32_t pos, double min_value) {
+   const uint32_t idx = src_index ? src_index[pos] : pos;
+   if (idx == NO_BLOCK) return false;
+   if (content) return content[pos] != 0;
+   return block_has_content(data + (size_t)idx * WID3, min_value);
+}
+
 __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
-   const uint8_t* __restrict__ content, const float* __restrict__ data, uint32_t* __restrict__ out_gids,
-   uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots, double* __restrict__ loss,
-   uint32_t* __restrict__ status, SweepCounters* __restrict__ counters, uint32_t out_capacity, MeshDev mesh,
-   double min_value, int add_width, double dv3) {
+   const uint8_t* __restrict__ content, const float* __restrict__ data, const int32_t* __restrict__ neighbors,
+   uint32_t* __restrict__ out_gids, uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots,
+   double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
+   uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
-   __shared__ int s_box[4];
+   __shared__ int s_box[8];
    __shared__ uint32_t s_base, s_flags;
    __shared__ double s_loss[ADJ_THREADS / 32];
 
@@ -93,20 +104,19 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    const CellSlot s = slots[cell];
    const uint32_t L0 = mesh.len[0], L1 = mesh.len[1], L2 = mesh.len[2];
    if (threadIdx.x == 0) {
-      s_box[0] = 1 << 20; s_box[1] = -1; s_box[2] = 1 << 20; s_box[3] = -1;
+      for (int q = 0; q < 8; q += 2) {
+         s_box[q] = 1 << 20;
+         s_box[q + 1] = -1;
+      }
       s_flags = 0;
    }
    __syncthreads();
-   // pass 1: bounding box (y, z) of the content blocks
+   // pass 1: bounding boxes (y, z) of the cell's content blocks and of its
+   // spatial neighbours' content blocks
    {
       int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
       for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-         const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-         bool c;
-         if (idx == NO_BLOCK) c = false;
-         else if (content) c = content[s.off + b] != 0;
-         else c = block_has_content(data + (size_t)idx * WID3, min_value);
-         if (c) {
+         if (list_block_content(src_index, content, data, s.off + b, min_value)) {
             const uint32_t g = gids[s.off + b];
             const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
             y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
@@ -114,13 +124,37 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       }
       atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
       atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
+      if (neighbors) {
+         int ny0 = 1 << 20, ny1 = -1, nz0 = 1 << 20, nz1 = -1;
+         for (int q = 0; q < 26; ++q) {
+            const int32_t nc = neighbors[(size_t)cell * 26 + q];
+            if (nc < 0) continue;
+            const CellSlot ns = slots[nc];
+            for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
+               if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
+                  const uint32_t g = gids[ns.off + b];
+                  const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+                  ny0 = min(ny0, y); ny1 = max(ny1, y); nz0 = min(nz0, z); nz1 = max(nz1, z);
+               }
+            }
+         }
+         atomicMin(&s_box[4], ny0); atomicMax(&s_box[5], ny1);
+         atomicMin(&s_box[6], nz0); atomicMax(&s_box[7], nz1);
+      }
    }
    __syncthreads();
-   const bool any = s_box[1] >= 0;
-   const int y0 = any ? max(0, s_box[0] - add_width) : 0;
-   const int y1 = any ? min((int)L1 - 1, s_box[1] + add_width) : -1;
-   const int z0 = any ? max(0, s_box[2] - add_width) : 0;
-   const int z1 = any ? min((int)L2 - 1, s_box[3] + add_width) : -1;
+   const bool own_any = s_box[1] >= 0, nb_any = s_box[5] >= 0;
+   const bool any = own_any || nb_any;
+   int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
+   if (own_any) {
+      y0 = max(0, s_box[0] - add_width); y1 = min((int)L1 - 1, s_box[1] + add_width);
+      z0 = max(0, s_box[2] - add_width); z1 = min((int)L2 - 1, s_box[3] + add_width);
+   }
+   if (nb_any) {
+      y0 = min(y0, s_box[4]); y1 = max(y1, s_box[5]);
+      z0 = min(z0, s_box[6]); z1 = max(z1, s_box[7]);
+   }
+   if (!any) { y0 = 0; y1 = -1; z0 = 0; z1 = -1; }
    const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
    const uint32_t rows = any ? (uint32_t)(ny * nz) : 0u;
    uint32_t* C = smem;              // 3 * rows
@@ -130,12 +164,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    __syncthreads();
    // pass 2: content mask rows
    for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-      bool c;
-      if (idx == NO_BLOCK) c = false;
-      else if (content) c = content[s.off + b] != 0;
-      else c = block_has_content(data + (size_t)idx * WID3, min_value);
-      if (c) {
+      if (list_block_content(src_index, content, data, s.off + b, min_value)) {
          const uint32_t g = gids[s.off + b];
          const uint32_t x = g % L0;
          const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
@@ -148,7 +177,6 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    const uint32_t xmask2 = (L0 >= 96) ? 0xffffffffu : ((L0 <= 64) ? 0u : ((1u << (L0 - 64)) - 1u));
    const uint32_t xmask1 = (L0 >= 64) ? 0xffffffffu : ((L0 <= 32) ? 0u : ((1u << (L0 - 32)) - 1u));
    const uint32_t xmask0 = (L0 >= 32) ? 0xffffffffu : ((1u << L0) - 1u);
-   uint32_t my_count = 0;
    const uint32_t chunk = (rows + blockDim.x - 1) / blockDim.x;
    const uint32_t r0 = min(rows, threadIdx.x * chunk), r1 = min(rows, r0 + chunk);
    for (uint32_t r = r0; r < r1; ++r) {
@@ -172,8 +200,29 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       }
       h0 &= xmask0; h1 &= xmask1; h2 &= xmask2;
       H[3 * r] = h0; H[3 * r + 1] = h1; H[3 * r + 2] = h2;
-      my_count += __popc(h0) + __popc(h1) + __popc(h2);
    }
+   __syncthreads();
+   // blocks with content in a spatial neighbour (adjust_velocity_blocks,
+   // spatial_cell_cpu.cpp:211-221)
+   if (neighbors && nb_any) {
+      for (int q = 0; q < 26; ++q) {
+         const int32_t nc = neighbors[(size_t)cell * 26 + q];
+         if (nc < 0) continue;
+         const CellSlot ns = slots[nc];
+         for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
+            if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
+               const uint32_t g = gids[ns.off + b];
+               const uint32_t x = g % L0;
+               const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+               const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+               atomicOr(&H[3 * r + (x >> 5)], 1u << (x & 31));
+            }
+         }
+      }
+      __syncthreads();
+   }
+   uint32_t my_count = 0;
+   for (uint32_t r = r0; r < r1; ++r) my_count += __popc(H[3 * r]) + __popc(H[3 * r + 1]) + __popc(H[3 * r + 2]);
    uint32_t total;
    uint32_t base_r = adj_exclusive_scan(my_count, warp_sums, total);
    for (uint32_t r = r0; r < r1; ++r) {
@@ -248,7 +297,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
 size_t adjust_smem_bytes(const MeshDev& mesh) { return sizeof(uint32_t) * 7 * mesh.len[1] * mesh.len[2] + 16; }
 
 cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const CellSlot* slots,
-                          const uint8_t* content, const float* data, uint32_t* out_gids, uint32_t* out_src,
+                          const uint8_t* content, const float* data, const int32_t* neighbors, uint32_t* out_gids,
+                          uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
                           uint32_t n_cells, cudaStream_t stream) {
@@ -256,9 +306,9 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
    const size_t smem = adjust_smem_bytes(mesh);
    cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    if (e != cudaSuccess) return e;
-   adjust_kernel<<<n_cells, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, out_gids, out_src,
-                                                          out_slots, loss, status, counters, out_capacity, mesh,
-                                                          min_value, add_width, dv3);
+   adjust_kernel<<<n_cells, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
+                                                          out_src, out_slots, loss, status, counters, out_capacity,
+                                                          mesh, min_value, add_width, dv3);
    return cudaGetLastError();
 }
 

@@ -43,10 +43,15 @@ cudaError_t launch_geometry(const CellAccelInputs* in, const double* moments, do
                             const double vmin[3], const double dv[3], uint32_t map_order, float threshold,
                             cudaStream_t stream);
 cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const CellSlot* slots,
-                          const uint8_t* content, const float* data, uint32_t* out_gids, uint32_t* out_src,
+                          const uint8_t* content, const float* data, const int32_t* neighbors, uint32_t* out_gids,
+                          uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
                           uint32_t n_cells, cudaStream_t stream);
+cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const CellAccelInputs* in, const MeshDev& mesh,
+                          const double vmin[3], const double bs[3], const double dv[3], const double dx[3], double q,
+                          double m, double max_rotation_deg, double* r_dt, double* v_dt, uint32_t n_cells,
+                          cudaStream_t stream);
 cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
                                cudaStream_t stream);
 struct TransCounters {
@@ -121,6 +126,9 @@ struct vlgpu_batch {
    uint32_t* trans_rows = nullptr;
    uint64_t row_cap = 0;
    TransCounters* tcounters = nullptr;
+   int32_t* neighbors = nullptr;  // 26 per cell (-1: none), the spatial neighbours block adjustment consults
+   double* dt_buf = nullptr;      // 2 per cell: r-space and v-space time-step limits
+   double* moments_r = nullptr;   // MOM_COUNT per cell: the moments after translation (the "_R" set)
    // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;
    CellAccelInputs* h_accel = nullptr;
@@ -174,6 +182,9 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->item_pencil);
    cudaFree(b->trans_rows);
    cudaFree(b->tcounters);
+   cudaFree(b->neighbors);
+   cudaFree(b->dt_buf);
+   cudaFree(b->moments_r);
    for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
    cudaFreeHost(b->h_sweep);
    cudaFreeHost(b->h_accel);
@@ -257,10 +268,11 @@ int run_sweep(vlgpu_batch* b, const double* intersections, size_t stride, uint32
    return sweep_device(b, b->sweep_cells, dim, per_cell, false);
 }
 
-int moments_device(vlgpu_batch* b, bool second) {
+int moments_device(vlgpu_batch* b, bool second, double* record = nullptr) {
    b->launches += 1;
-   VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, b->moments, b->mdev, b->vmin_d,
-                           b->bs_d, b->dv_d, b->params.mass, b->params.charge, second, b->n_cells, b->stream));
+   VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, record ? record : b->moments,
+                           b->mdev, b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, second,
+                           b->n_cells, b->stream));
    return VLGPU_OK;
 }
 
@@ -270,7 +282,8 @@ int adjust_device(vlgpu_batch* b) {
    VL_CHECK(cudaMemsetAsync(b->counters, 0, sizeof(SweepCounters), b->stream));
    const double dv3 = b->dv_d[0] * b->dv_d[1] * b->dv_d[2];
    VL_CHECK(launch_adjust(b->st_gids, b->st_src, b->st_slots, b->content_valid ? b->content : nullptr,
-                          b->data[b->cur], b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss, b->status,
+                          b->data[b->cur], b->neighbors, b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss,
+                          b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
                           (int)b->params.add_width_v, dv3, b->n_cells, b->stream));
    b->launches += 1;
@@ -344,6 +357,22 @@ int translate_device(vlgpu_batch* b, uint32_t dim, double dt) {
    set_direct_state(b, d);
    b->content_valid = false;
    return VLGPU_OK;
+}
+
+// One full Vlasov step of a grid: translation z, x, y and the "_R" moments
+// (calculateSpatialTranslation, vlasovmover.cpp:65-381), then one acceleration
+// step with its final adjustment and "_V" moments (calculateAcceleration,
+// vlasovmover.cpp:410-581), as the reference's main loop orders them.
+int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order) {
+   static const uint32_t trans_order[3] = {2, 0, 1};
+   for (int s = 0; s < 3; ++s) {
+      const int st = translate_device(b, trans_order[s], dt);
+      if (st != VLGPU_OK) return st;
+   }
+   int st = moments_device(b, false, b->moments_r);
+   if (st == VLGPU_OK) st = moments_device(b, true, b->moments_r);
+   if (st != VLGPU_OK) return st;
+   return accelerate_device(b, map_order, false);
 }
 
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
@@ -716,6 +745,29 @@ int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx
       VL_CHECK(cudaMalloc(&b->tcounters, sizeof(TransCounters)));
       VL_CHECK(cudaMemset(b->tcounters, 0, sizeof(TransCounters)));
    }
+   // the 26 nearest neighbours of every cell, periodic, the cell itself excluded
+   std::vector<int32_t> nb((size_t)b->n_cells * 26);
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      const int x = (int)(c % dims[0]), y = (int)((c / dims[0]) % dims[1]), z = (int)(c / (dims[0] * dims[1]));
+      int q = 0;
+      for (int dz = -1; dz <= 1; ++dz)
+         for (int dy = -1; dy <= 1; ++dy)
+            for (int dx_ = -1; dx_ <= 1; ++dx_) {
+               if (dx_ == 0 && dy == 0 && dz == 0) continue;
+               const int xx = (x + dx_ + (int)dims[0]) % (int)dims[0];
+               const int yy = (y + dy + (int)dims[1]) % (int)dims[1];
+               const int zz = (z + dz + (int)dims[2]) % (int)dims[2];
+               const uint32_t n = (uint32_t)xx + dims[0] * ((uint32_t)yy + dims[1] * (uint32_t)zz);
+               nb[(size_t)c * 26 + q++] = (n == c) ? -1 : (int32_t)n;
+            }
+   }
+   if (!b->neighbors) VL_CHECK(cudaMalloc(&b->neighbors, sizeof(int32_t) * nb.size()));
+   if (!b->dt_buf) VL_CHECK(cudaMalloc(&b->dt_buf, sizeof(double) * 2 * b->n_cells));
+   if (!b->moments_r) {
+      VL_CHECK(cudaMalloc(&b->moments_r, sizeof(double) * MOM_COUNT * b->n_cells));
+      VL_CHECK(cudaMemset(b->moments_r, 0, sizeof(double) * MOM_COUNT * b->n_cells));
+   }
+   VL_CHECK(cudaMemcpy(b->neighbors, nb.data(), sizeof(int32_t) * nb.size(), cudaMemcpyHostToDevice));
    for (int d = 0; d < 3; ++d) {
       b->grid_dims[d] = dims[d];
       b->grid_dx[d] = dx[d];
@@ -728,6 +780,44 @@ int vlgpu_translate(vlgpu_batch* b, uint32_t dimension, double dt) {
    if (!b || dimension > 2 || !b->has_grid) return VLGPU_EINVAL;
    VL_CHECK(cudaSetDevice(b->device));
    return translate_device(b, dimension, dt);
+}
+
+int vlgpu_vlasov_step(vlgpu_batch* b, const vlgpu_cell_fields* fields, double dt, uint32_t map_order) {
+   if (!b || !fields || map_order > 2 || !b->has_grid) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   const std::vector<double> dts(b->n_cells, dt);
+   const int st = stage_fields(b, fields, dts.data());
+   if (st != VLGPU_OK) return st;
+   return vlasov_step_device(b, dt, map_order);
+}
+
+int vlgpu_vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order) {
+   if (!b || map_order > 2 || !b->has_grid) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   return vlasov_step_device(b, dt, map_order);
+}
+
+int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16) {
+   if (!b || !out16 || !b->moments_r) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaMemcpyAsync(out16, b->moments_r, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
+                            b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_max_dt(vlgpu_batch* b, double max_rotation_deg, double* r_dt, double* v_dt) {
+   if (!b || !r_dt || !v_dt || !b->has_grid) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   double* d = b->dt_buf;
+   cudaError_t e = launch_max_dt(b->st_gids, b->st_slots, b->accel_in, b->mdev, b->vmin_d, b->bs_d, b->dv_d,
+                                 b->grid_dx, b->params.charge, b->params.mass, max_rotation_deg, d, d + b->n_cells,
+                                 b->n_cells, b->stream);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(r_dt, d, sizeof(double) * b->n_cells, cudaMemcpyDeviceToHost, b->stream);
+   if (e == cudaSuccess)
+      e = cudaMemcpyAsync(v_dt, d + b->n_cells, sizeof(double) * b->n_cells, cudaMemcpyDeviceToHost, b->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+   return cuda_status(e, "vlgpu_batch_max_dt");
 }
 
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact) {

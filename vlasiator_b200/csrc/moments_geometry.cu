@@ -263,6 +263,61 @@ __global__ void geometry_kernel(const CellAccelInputs* __restrict__ in, const do
 }
 
 // ---------------------------------------------------------------------------
+// Time-step limits per cell: the r-space limit of reduce_vlasov_dt
+// (vlasovsolver/arch_dt.cpp:34-97), min over blocks and over the first and
+// last cell of the block of min(dx/|vx|, dy/|vy|, dz/|vz|) at those cells'
+// centres (+1000*DBL_MIN), and the v-space limit of updateAccelerationMaxdt
+// (cpu_acc_transform.cpp:41-55), |gyroperiod| * max_rotation/360.
+// ---------------------------------------------------------------------------
+constexpr int DT_THREADS = 128;
+
+__global__ void __launch_bounds__(DT_THREADS) max_dt_kernel(
+   const uint32_t* __restrict__ gids, const CellSlot* __restrict__ slots, const CellAccelInputs* __restrict__ in,
+   MeshDev mesh, double vmin0, double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1,
+   double dv2, double dx, double dy, double dz, double q, double m, double max_rotation_deg, double* __restrict__ r_dt,
+   double* __restrict__ v_dt) {
+   __shared__ double s_min[DT_THREADS / 32];
+   const uint32_t cell = blockIdx.x;
+   const CellSlot s = slots[cell];
+   const double EPS = 2.2250738585072014e-308 * 1000;  // numeric_limits<Real>::min() * 1000
+   double t = 1.7976931348623157e308;
+   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+      const uint32_t g = gids[s.off + b];
+      const uint32_t bi = g % mesh.len[0], bj = (g / mesh.len[0]) % mesh.len[1], bk = g / (mesh.len[0] * mesh.len[1]);
+      const double cx = vmin0 + bi * bs0, cy = vmin1 + bj * bs1, cz = vmin2 + bk * bs2;
+      for (int i = 0; i < WID; i += WID - 1) {
+         const double Vx = cx + (i + 0.5) * dv0 + EPS;
+         const double Vy = cy + (i + 0.5) * dv1 + EPS;
+         const double Vz = cz + (i + 0.5) * dv2 + EPS;
+         t = fmin(t, fmin(dx / fabs(Vx), fmin(dy / fabs(Vy), dz / fabs(Vz))));
+      }
+   }
+#pragma unroll
+   for (int o = 16; o >= 1; o >>= 1) t = fmin(t, __shfl_xor_sync(0xffffffffu, t, o));
+   if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = t;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int w = 1; w < DT_THREADS / 32; ++w) t = fmin(t, s_min[w]);
+      r_dt[cell] = t;
+      const CellAccelInputs a = in[cell];
+      const double B_mag = sqrt(a.B[0] * a.B[0] + a.B[1] * a.B[1] + a.B[2] * a.B[2]) + 1e-30;
+      const double gyro_period = 2 * M_PI * m / (q * B_mag);
+      v_dt[cell] = fabs(gyro_period) * (max_rotation_deg / 360.0);
+   }
+}
+
+cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const CellAccelInputs* in, const MeshDev& mesh,
+                          const double vmin[3], const double bs[3], const double dv[3], const double dx[3], double q,
+                          double m, double max_rotation_deg, double* r_dt, double* v_dt, uint32_t n_cells,
+                          cudaStream_t stream) {
+   if (n_cells == 0) return cudaSuccess;
+   max_dt_kernel<<<n_cells, DT_THREADS, 0, stream>>>(gids, slots, in, mesh, vmin[0], vmin[1], vmin[2], bs[0], bs[1],
+                                                     bs[2], dv[0], dv[1], dv[2], dx[0], dx[1], dx[2], q, m,
+                                                     max_rotation_deg, r_dt, v_dt);
+   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
                            double* moments,
                            const MeshDev& mesh, const double vmin[3], const double bs[3], const double dv[3],

@@ -144,3 +144,21 @@ def random_drifting_cells(n_cells: int, seed: int = 0, mesh: VelocityMesh | None
         c.B = B
         cells.append(c)
     return cells
+
+
+def sinewave_grid(dims, mesh: VelocityMesh | None = None, n0: float = 1e6, amplitude: float = 0.5, T: float = 1e6,
+                  V=(4e5, 0.0, 0.0), B=(0.0, 0.0, 5e-9), min_value: float = 1e-15):
+    """The full-Vlasov-step workload on a uniform periodic grid (cells x
+    fastest): a Maxwellian per cell with n = n0 (1 + amplitude sin(2 pi x / Lx)),
+    temperature T, bulk velocity V and uniform B, as the sine-wave translation
+    tests of the reference set it up (testpackage transtest_2_amr_sinewave, on
+    a uniform grid).  Cells with equal density share one generated VDF."""
+    mesh = mesh or VelocityMesh()
+    nx, ny, nz = (int(v) for v in dims)
+    by_x = []
+    for x in range(nx):
+        n = n0 * (1.0 + amplitude * np.sin(2.0 * np.pi * x / nx))
+        c = maxwellian_cell(mesh, n, T, V, min_value=min_value)
+        c.B = np.asarray(B, np.float64)
+        by_x.append(c)
+    return [by_x[c % nx] for c in range(nx * ny * nz)]

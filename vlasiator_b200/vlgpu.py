@@ -85,6 +85,10 @@ SIGNATURES = {
     "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_set_grid": (ctypes.c_int, [_vp, _u32p, _dp]),
     "vlgpu_translate": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_double]),
+    "vlgpu_batch_max_dt": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp]),
+    "vlgpu_vlasov_step": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), ctypes.c_double, ctypes.c_uint32]),
+    "vlgpu_vlasov_step_device": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_uint32]),
+    "vlgpu_batch_moments_r": (ctypes.c_int, [_vp, _dp]),
     "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
                                             _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
                                             _u32p, _vp]),
@@ -278,6 +282,27 @@ class Batch:
     def translate(self, dim: int, dt: float):
         """One translation sweep (trans_map_1d_amr) along dim over dt seconds."""
         _check(self.lib.vlgpu_translate(self.h, dim, float(dt)), "vlgpu_translate")
+
+    def vlasov_step(self, B, dt: float, map_order: int, curl=None, egradpe=None):
+        """Translation z, x, y + "_R" moments, then one acceleration step (grid batches)."""
+        F, _ = self._fields(B, dt, curl, egradpe)
+        _check(self.lib.vlgpu_vlasov_step(self.h, F, float(dt), map_order), "vlgpu_vlasov_step")
+
+    def vlasov_step_device(self, dt: float, map_order: int):
+        _check(self.lib.vlgpu_vlasov_step_device(self.h, float(dt), map_order), "vlgpu_vlasov_step_device")
+
+    def moments_r(self) -> np.ndarray:
+        out = np.zeros((self.n_cells, 16))
+        _check(self.lib.vlgpu_batch_moments_r(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_moments_r")
+        return out
+
+    def max_dt(self, max_rotation_deg: float = 22.0):
+        """(r_dt, v_dt) per cell: reduce_vlasov_dt and updateAccelerationMaxdt limits."""
+        r = np.zeros(self.n_cells)
+        v = np.zeros(self.n_cells)
+        _check(self.lib.vlgpu_batch_max_dt(self.h, float(max_rotation_deg), _p(r, ctypes.c_double),
+                                           _p(v, ctypes.c_double)), "vlgpu_batch_max_dt")
+        return r, v
 
     def adjust(self):
         _check(self.lib.vlgpu_adjust_blocks(self.h), "vlgpu_adjust_blocks")
