@@ -455,6 +455,75 @@ def run_vlasov(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# serving: a Poisson stream of independent VDF-advance requests
+# ---------------------------------------------------------------------------
+SERVE_WORKLOAD = ("serving: Poisson stream of {n} independent requests ({distinct} distinct drifting bi-Maxwellian "
+                  "VDFs, T_par/T_perp U(0.5,3), blocks log-normal median 5k clipped 500..60k; own B 5-50 nT, "
+                  "E=-VxB, dt=0.01 gyroperiod, steps U(1,{max_steps})); {budget} GB HBM budget, state device-resident")
+
+
+def run_serve(args):
+    world, rank, local, pg = dist_setup()
+    from vlasiator_b200 import vlgpu
+    vlgpu.load()
+    import torch
+    torch.cuda.set_device(local)
+    from vlasiator_b200.projects import serving_requests
+    from vlasiator_b200.serve import Server, run_plain, run_stream
+    mesh = VelocityMesh()
+    base = serving_requests(args.distinct, seed=args.seed + rank, mesh=mesh, max_steps=args.max_steps)
+    rng = np.random.default_rng(args.seed + 17 + rank)
+    reqs = []
+    for k in range(args.requests):
+        q = dict(base[k % len(base)])
+        q["steps"] = int(rng.integers(1, args.max_steps + 1))
+        reqs.append(q)
+    work = sum(WID3 * q["cell"].n_blocks * q["steps"] for q in reqs)  # nominal, blocks at submission
+    budget = int(args.budget_gb * 1e9)
+    with Server(mesh, args.max_cells, budget, device=local) as srv:
+        # warm-up: a few requests through the whole path
+        run_stream(srv, reqs[: min(8, len(reqs))], rate_per_s=1e6)
+        st0 = srv.stats()
+        if pg is not None:
+            pg.barrier()
+        with ClockSampler(local) as clk:
+            latency, wall, _ = run_stream(srv, reqs, rate_per_s=args.rate, seed=args.seed)
+        st1 = srv.stats()
+    updates = st1["cell_updates"] - st0["cell_updates"]
+    wall_max = allreduce_max(pg, wall)
+    value = allreduce_sum(pg, float(updates)) / wall_max
+    # the plain per-request launch path on a bounded sample of the same requests
+    plain = None
+    if args.plain_requests > 0:
+        sample = reqs[: args.plain_requests]
+        times, _ = run_plain(mesh, sample)
+        p_work = sum(WID3 * q["cell"].n_blocks * q["steps"] for q in sample)
+        p_value = p_work / float(times.sum())
+        plain = {"value": p_value, "unit": UNIT, "requests": len(sample), "seconds": float(times.sum()),
+                 "latency_p50_ms": float(np.percentile(times, 50) * 1e3),
+                 "served_over_plain": value / p_value,
+                 "path": "one request at a time: vlgpu_batch_upload + vlgpu_accelerate_per_cell x steps + download"}
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(reqs), "warmup": 8,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded bi-Maxwellian requests)",
+        "config": {"workload": SERVE_WORKLOAD.format(n=len(reqs), distinct=len(base), max_steps=args.max_steps,
+                                                     budget=args.budget_gb),
+                   "arrival_rate_per_s": args.rate, "max_cells": args.max_cells,
+                   "nominal_cell_updates": work, "wall_s": wall_max},
+        "latency_ms": {"p50": float(np.percentile(latency, 50) * 1e3),
+                       "p99": float(np.percentile(latency, 99) * 1e3),
+                       "what": "request arrival to its result on the host (wall clock)"},
+        "plain_per_request": plain,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,14 +538,23 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--exact", action="store_true", help="remap in the reference's exact operation order")
     ap.add_argument("--plain-steps", type=int, default=2, help="steps of the plain per-cell path (0: skip)")
-    ap.add_argument("--workload", default="accel", choices=["accel", "vlasov"],
+    ap.add_argument("--workload", default="accel", choices=["accel", "vlasov", "serve"],
                     help="accel: batched acceleration of independent cells; vlasov: full step of a periodic grid")
     ap.add_argument("--grid", type=int, nargs=3, default=[64, 64, 16], help="grid of the vlasov workload")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
+    ap.add_argument("--distinct", type=int, default=100, help="serve: distinct generated VDFs")
+    ap.add_argument("--max-steps", type=int, default=100, help="serve: steps per request U(1, max)")
+    ap.add_argument("--rate", type=float, default=400.0, help="serve: mean arrival rate (requests/s)")
+    ap.add_argument("--max-cells", type=int, default=4096, help="serve: cells of the server's batch")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget (GB)")
+    ap.add_argument("--plain-requests", type=int, default=8, help="serve: requests timed on the plain path")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "vlasov":
         return run_vlasov(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -29,6 +29,7 @@ extern "C" {
 #define VLGPU_ERANGE 5    /* a column's target window exceeded the remap ring (rotation per step too large) */
 #define VLGPU_ECUDA 6     /* CUDA runtime error */
 #define VLGPU_ENODEV 7    /* no CUDA device */
+#define VLGPU_EAGAIN 8    /* a served request has not finished yet */
 
 #define VLGPU_CELL_WALL 1u
 #define VLGPU_CELL_RANGE 2u
@@ -271,6 +272,47 @@ int vlgpu_batch_set_exact(vlgpu_batch* b, int exact);
 
 /* Synchronises the batch's stream and returns the first error seen. */
 int vlgpu_batch_sync(vlgpu_batch* b);
+
+/* ---- serving ------------------------------------------------------------ */
+
+/* A request loop around one device-resident batch of max_cells cells: each
+   request is one spatial cell's VDF to be advanced by n_steps acceleration
+   steps (calculateAcceleration for one population, as vlgpu_accelerate does
+   it).  Requests queue on the host, join the batch between steps while free
+   cells and the block budget allow (continuous batching), keep their blocks
+   on the device for their whole life and are copied back after their last
+   step.  hbm_budget_bytes sizes the batch: block capacity = budget / bytes
+   per block of all the batch's arrays; admission keeps the live blocks below
+   60% of it.  Step s of every request uses dimension order s mod 3 and cells
+   never interact, so a request's result does not depend on the requests it
+   ran with.  One host thread drives a server. */
+typedef struct vlgpu_server vlgpu_server;
+int vlgpu_server_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint32_t max_cells,
+                        uint64_t hbm_budget_bytes, int device, vlgpu_server** out);
+int vlgpu_server_destroy(vlgpu_server* s);
+
+/* Queues a request (its data are copied); *request_id identifies it. */
+int vlgpu_server_submit(vlgpu_server* s, uint32_t n_blocks, const uint32_t* gids, const float* data,
+                        const vlgpu_cell_fields* fields, double dt, uint32_t n_steps, uint64_t* request_id);
+
+/* One tick: waits for the previous step, copies finished requests back,
+   admits queued ones, and issues one acceleration step of all active cells
+   (asynchronously).  Reports the active, queued and just-finished counts. */
+int vlgpu_server_tick(vlgpu_server* s, uint32_t* n_active, uint32_t* n_pending, uint32_t* n_done);
+
+/* The result of a finished request (blocks in ascending global-ID order, its
+   VLGPU_CELL_* bits and its block-adjustment loss), then forgets it.
+   VLGPU_EAGAIN while it runs; VLGPU_ENOMEM (with *n_blocks set) when
+   capacity is too small. */
+int vlgpu_server_result(vlgpu_server* s, uint64_t request_id, uint32_t* n_blocks, uint32_t* gids, float* data,
+                        uint64_t capacity, uint32_t* status, double* rho_loss);
+
+/* [0] ticks, [1] requests finished, [2] cell-steps run, [3] phase-space
+   cell-updates (64 x blocks entering each step). */
+int vlgpu_server_stats(vlgpu_server* s, uint64_t* out4);
+
+/* The server's batch (for its stream and counters; do not destroy it). */
+int vlgpu_server_batch(vlgpu_server* s, vlgpu_batch** batch);
 
 /* Library version string. */
 const char* vlgpu_version(void);

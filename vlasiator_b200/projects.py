@@ -162,3 +162,60 @@ def sinewave_grid(dims, mesh: VelocityMesh | None = None, n0: float = 1e6, ampli
         c.B = np.asarray(B, np.float64)
         by_x.append(c)
     return [by_x[c % nx] for c in range(nx * ny * nz)]
+
+
+def _bimaxwellian_blocks(mesh: VelocityMesh, n: float, T_perp: float, T_par: float, min_value: float) -> float:
+    """Estimated block count (content plus its +-1 halo) of a bi-Maxwellian."""
+    peak = n * (MASS_PROTON / (2.0 * np.pi * K_B)) ** 1.5 / (T_perp * np.sqrt(T_par))
+    if peak <= min_value:
+        return 0.0
+    lg = np.log(peak / min_value)
+    r_perp = np.sqrt(2.0 * K_B * T_perp / MASS_PROTON * lg) / mesh.block_size[0]
+    r_par = np.sqrt(2.0 * K_B * T_par / MASS_PROTON * lg) / mesh.block_size[0]
+    return 4.0 / 3.0 * np.pi * (r_perp + 1.0) ** 2 * (r_par + 1.0)
+
+
+def serving_requests(n_requests: int, seed: int = 0, mesh: VelocityMesh | None = None, max_steps: int = 100,
+                     min_value: float = 1e-15):
+    """Independent VDF-advance requests of the serving workload.
+
+    Each: a drifting bi-Maxwellian (tri-Maxwellian of projects/project.h:66-73
+    with T_x = T_y = T_perp in the magnetic-field frame), T_par / T_perp
+    uniform in [0.5, 3], n = 1e6 m^-3, |V| uniform in [0, 800] km/s along a
+    random direction; its block count drawn log-normal (median 5000, clipped
+    to 500..60000) and met by choosing T_perp; B of random direction with |B|
+    uniform in [5, 50] nT (E = -V x B enters through the gyration about V);
+    dt = 0.01 gyroperiod; steps uniform in 1..max_steps.
+    Returns dicts with keys cell (CellState), B, dt, steps."""
+    from .mesh import CHARGE
+    mesh = mesh or VelocityMesh()
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_requests):
+        target = float(np.clip(np.exp(rng.normal(np.log(5000.0), 0.8)), 500.0, 60000.0))
+        est = target / 1.35  # the ellipsoid-plus-halo estimate runs about 35% below the pruned count
+        ratio = rng.uniform(0.5, 3.0)
+        n = 1e6
+        lo, hi = 1e3, 1e9
+        for _ in range(60):  # bisection on T_perp for the target block count
+            mid = np.sqrt(lo * hi)
+            if _bimaxwellian_blocks(mesh, n, mid, ratio * mid, min_value) < est:
+                lo = mid
+            else:
+                hi = mid
+        T_perp = np.sqrt(lo * hi)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        V = d * rng.uniform(0.0, 8.0e5)
+        b = rng.normal(size=3)
+        b /= np.linalg.norm(b)
+        Bmag = rng.uniform(5e-9, 50e-9)
+        e1 = np.cross(b, [1.0, 0.0, 0.0] if abs(b[0]) < 0.9 else [0.0, 1.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(b, e1)
+        R = np.stack([e1, e2, b])
+        cell = maxwellian_cell(mesh, n, T_perp, V, min_value, T_aniso=(T_perp, T_perp, ratio * T_perp, R))
+        cell.B = b * Bmag
+        Tg = 2.0 * np.pi * MASS_PROTON / (CHARGE * Bmag)
+        out.append({"cell": cell, "B": cell.B, "dt": 0.01 * Tg, "steps": int(rng.integers(1, max_steps + 1))})
+    return out

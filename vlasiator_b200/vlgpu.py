@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvlgpu.so")
 
 STATUS = {0: "VLGPU_OK", 1: "VLGPU_EINVAL", 2: "VLGPU_ENOMEM", 3: "VLGPU_EWALL", 4: "VLGPU_ETIMEDOUT",
-          5: "VLGPU_ERANGE", 6: "VLGPU_ECUDA", 7: "VLGPU_ENODEV"}
+          5: "VLGPU_ERANGE", 6: "VLGPU_ECUDA", 7: "VLGPU_ENODEV", 8: "VLGPU_EAGAIN"}
 CELL_WALL, CELL_RANGE, CELL_NOMEM, CELL_BADDK = 1, 2, 4, 8
 
 
@@ -89,6 +89,15 @@ SIGNATURES = {
     "vlgpu_vlasov_step": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), ctypes.c_double, ctypes.c_uint32]),
     "vlgpu_vlasov_step_device": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_uint32]),
     "vlgpu_batch_moments_r": (ctypes.c_int, [_vp, _dp]),
+    "vlgpu_server_create": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32,
+                                           ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "vlgpu_server_destroy": (ctypes.c_int, [_vp]),
+    "vlgpu_server_submit": (ctypes.c_int, [_vp, ctypes.c_uint32, _u32p, _fp, ctypes.POINTER(CFieldsT),
+                                           ctypes.c_double, ctypes.c_uint32, _u64p]),
+    "vlgpu_server_tick": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
+    "vlgpu_server_result": (ctypes.c_int, [_vp, ctypes.c_uint64, _u32p, _u32p, _fp, ctypes.c_uint64, _u32p, _dp]),
+    "vlgpu_server_stats": (ctypes.c_int, [_vp, _u64p]),
+    "vlgpu_server_batch": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
                                             _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
                                             _u32p, _vp]),
