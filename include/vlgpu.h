@@ -270,6 +270,19 @@ int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out);
    is conserved as in the exact mode. */
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact);
 
+/* Selects the acceleration reconstruction of later sweeps, the reference's
+   compile-time ACC_SEMILAG_* choice (cpu_acc_map.cpp:537-548, 590-601):
+   VLGPU_RECON_PLM (compute_plm_coeff, cpu_1d_plm.hpp:38-49), VLGPU_RECON_PPM
+   (the default; compute_ppm_coeff, cpu_1d_ppm.hpp:35-54) or VLGPU_RECON_PQM
+   (compute_pqm_coeff with h8 faces and h7 derivatives, cpu_1d_pqm.hpp:157-176,
+   cpu_face_estimates.hpp:45-79, 216-275; the reference Makefile's default).
+   PLM and PQM run in the fused arithmetic only (values within 1e-5 of the
+   cell's peak per sweep); combining them with exact = 1 is VLGPU_EINVAL. */
+#define VLGPU_RECON_PLM 1
+#define VLGPU_RECON_PPM 2
+#define VLGPU_RECON_PQM 4
+int vlgpu_batch_set_reconstruction(vlgpu_batch* b, int order);
+
 /* Synchronises the batch's stream and returns the first error seen. */
 int vlgpu_batch_sync(vlgpu_batch* b);
 

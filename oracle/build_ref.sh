@@ -8,6 +8,7 @@
 #
 #   oracle/_ref/libvlasov_ref_sp.so  : FP32 VDF (Realf=float, Real=double), VECL=16, PPM
 #   oracle/_ref/libvlasov_ref_dp.so  : all-FP64 (Realf=double), VECL=8, PPM
+#   oracle/_ref/libvlasov_ref_sp_pqm.so, libvlasov_ref_sp_plm.so : FP32, PQM / PLM acceleration
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -euo pipefail
@@ -48,7 +49,7 @@ cp "$HERE/ref_harness.cpp" "$SRC/ref_harness.cpp"
 
 CXX="${REF_CXX:-/usr/bin/g++}"
 COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
-        -DDP -DACC_SEMILAG_PPM -DTRANS_SEMILAG_PPM -DVEC_FALLBACK_GENERIC
+        -DDP -DTRANS_SEMILAG_PPM -DVEC_FALLBACK_GENERIC
         -I"$SRC" -I"$SRC/sysinc" -w)
 SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
       "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
@@ -57,6 +58,16 @@ SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
 CC="${REF_CC:-/usr/bin/gcc}"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_sp.o"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -DORC_DOUBLE -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_dp.o"
-"$CXX" "${COMMON[@]}" -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" -o "$OUT/libvlasov_ref_sp.so"
-"$CXX" "${COMMON[@]}" -DDPF -DVECL=8 "${SRCS[@]}" "$OUT/orc_geometry_dp.o" -o "$OUT/libvlasov_ref_dp.so"
-echo "build_ref: built $OUT/libvlasov_ref_sp.so $OUT/libvlasov_ref_dp.so"
+"$CXX" "${COMMON[@]}" -DACC_SEMILAG_PPM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
+  -o "$OUT/libvlasov_ref_sp.so" &
+"$CXX" "${COMMON[@]}" -DACC_SEMILAG_PPM -DDPF -DVECL=8 "${SRCS[@]}" "$OUT/orc_geometry_dp.o" \
+  -o "$OUT/libvlasov_ref_dp.so" &
+# the other acceleration reconstructions of the reference (PQM is its
+# Makefile default, PLM the lowest order), FP32 VDF
+"$CXX" "${COMMON[@]}" -DACC_SEMILAG_PQM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
+  -o "$OUT/libvlasov_ref_sp_pqm.so" &
+"$CXX" "${COMMON[@]}" -DACC_SEMILAG_PLM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
+  -o "$OUT/libvlasov_ref_sp_plm.so" &
+wait
+for f in sp dp sp_pqm sp_plm; do test -f "$OUT/libvlasov_ref_$f.so"; done
+echo "build_ref: built $OUT/libvlasov_ref_{sp,dp,sp_pqm,sp_plm}.so"

@@ -252,10 +252,13 @@ class ReferenceBuild:
     _mesh_set = {}
 
     def __init__(self, precision: str = "sp"):
+        """precision: "sp" / "dp" (PPM), or "sp_pqm" / "sp_plm" for the
+        reference's other acceleration reconstructions (FP32)."""
         path = os.path.join(HERE, "_ref", f"libvlasov_ref_{precision}.so")
         self.lib = ctypes.CDLL(path)
-        self.realf = np.float32 if precision == "sp" else np.float64
-        ct = ctypes.c_float if precision == "sp" else ctypes.c_double
+        sp = precision.startswith("sp")
+        self.realf = np.float32 if sp else np.float64
+        ct = ctypes.c_float if sp else ctypes.c_double
         self._ct = ct
         L = self.lib
         L.ref_init.argtypes = [_dp, _dp, _u32p, ctypes.c_uint32]

@@ -2,11 +2,13 @@
 
 Runs the reference's map_1d (vlasovsolver/cpu_acc_map.cpp:121-636, built by
 oracle/build_ref.sh into oracle/_ref/) on small seeded Maxwellian cells and
-stores inputs, intersections and outputs as compressed .npz files.  The
+stores inputs, intersections and outputs as compressed .npz files: PPM in
+FP32 and FP64 (map1d_sp, map1d_dp) and the PQM and PLM reconstructions in
+FP32 (map1d_sp_pqm, map1d_sp_plm).  The
 fixtures let the parity tests pin the oracle and the CUDA path on machines
 where the reference tree is not available.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--all]   (default: only missing files)
 """
 from __future__ import annotations
 
@@ -38,7 +40,7 @@ def make(precision: str = "sp") -> str:
     mesh = VelocityMesh()
     ref = ReferenceBuild(precision)
     ref.init(mesh)
-    orc = Restatement(precision)
+    orc = Restatement(precision[:2])
     cases = []
     c0 = larmor_cell()
     cases.append(("larmor", c0, 0.01, 0))
@@ -70,5 +72,6 @@ def make(precision: str = "sp") -> str:
 
 
 if __name__ == "__main__":
-    for p in ("sp", "dp"):
-        print(make(p))
+    for p in ("sp", "dp", "sp_pqm", "sp_plm"):
+        if "--all" in sys.argv or not os.path.exists(os.path.join(HERE, f"map1d_{p}.npz")):
+            print(make(p))

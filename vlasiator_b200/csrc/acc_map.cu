@@ -133,6 +133,121 @@ __device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, 
    a2 = fl + fr - 2.0f * v0;
 }
 
+// Superbee slope of (l, m, r) on unscaled values: sign(a) * max(min(|a|, 2|b|),
+// min(2|a|, |b|)) when a = r - m and b = m - l share a sign, else 0.
+__device__ __forceinline__ float superbee_fused(float l, float m, float r) {
+   const float a = r - m, b = m - l;
+   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const float aa = fabsf(a), ab = fabsf(b);
+   return same ? copysignf(fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)), a) : 0.0f;
+}
+
+// PLM coefficients (compute_plm_coeff, cpu_1d_plm.hpp:38-49): f = a0 + 2 a1 t.
+__device__ __forceinline__ void plm_coeff_fused(float vm1, float v0, float vp1, float a[5]) {
+   const float d = superbee_fused(vm1, v0, vp1);
+   a[0] = v0 - 0.5f * d;
+   a[1] = 0.5f * d;
+}
+
+// h8 face value and h7 face derivative of the left face of the cell whose
+// stencil is w0..w7 = values k-4 .. k+3 (cpu_face_estimates.hpp:45-79).
+__device__ __forceinline__ float h8_value(float w0, float w1, float w2, float w3, float w4, float w5, float w6,
+                                          float w7) {
+   return (float)(1.0 / 840.0) *
+          (533.0f * (w3 + w4) - 139.0f * (w2 + w5) + 29.0f * (w1 + w6) - 3.0f * (w0 + w7));
+}
+__device__ __forceinline__ float h7_derivative(float w0, float w1, float w2, float w3, float w4, float w5, float w6,
+                                               float w7) {
+   return (float)(1.0 / 5040.0) *
+          (7175.0f * (w4 - w3) - 889.0f * (w5 - w2) + 119.0f * (w6 - w1) - 9.0f * (w7 - w0));
+}
+
+// PQM coefficients (compute_pqm_coeff, cpu_1d_pqm.hpp:157-176) from the raw
+// h8/h7 faces: the extremum / boundedness / slope filters of
+// compute_filtered_face_values_derivatives (cpu_face_estimates.hpp:216-275)
+// and the inflexion-point filter filter_pqm_monotonicity (cpu_1d_pqm.hpp:
+// 31-156), in single precision.
+__device__ __forceinline__ void pqm_coeff_fused(float vm1, float v0, float vp1, float fv_l, float fv_r, float fd_l,
+                                                float fd_r, float a[5]) {
+   const float slope = superbee_fused(vm1, v0, vp1);
+   const float slope_abs = fabsf(slope);
+   const float slope_sign = slope > 0.0f ? 1.0f : -1.0f;
+   if (slope_abs == 0.0f) {
+      fv_r = v0;
+      fv_l = v0;
+      fd_l = 0.0f;
+      fd_r = 0.0f;
+   }
+   if ((vm1 - fv_l) * (fv_l - v0) < 0.0f || slope_sign * fd_l < 0.0f) {
+      fv_l = v0 - slope_sign * 0.5f * slope_abs;
+      fd_l = slope_sign * slope_abs;
+   }
+   if ((vp1 - fv_r) * (fv_r - v0) < 0.0f || slope_sign * fd_r < 0.0f) {
+      fv_r = v0 + slope_sign * 0.5f * slope_abs;
+      fd_r = slope_sign * slope_abs;
+   }
+   // second-derivative coefficients (White and Adcroft 2008, eq. 23)
+   const float b0 = 60.0f * v0 - 24.0f * fv_r - 36.0f * fv_l + 3.0f * (fd_r - 3.0f * fd_l);
+   const float b1 = -360.0f * v0 + 36.0f * fd_l - 24.0f * fd_r + 168.0f * fv_r + 192.0f * fv_l;
+   const float b2 = 360.0f * v0 + 30.0f * (fd_r - fd_l) - 180.0f * (fv_l + fv_r);
+   const float disc = b1 * b1 - 4.0f * b0 * b2;
+   const float sq = disc < 0.0f ? b1 + 200.0f * b2 : sqrtf(disc);
+   const float root1 = (-b1 + sq) / (2.0f * b2);
+   const float root2 = (-b1 - sq) / (2.0f * b2);
+   const float plm_l = 2.0f * (v0 - vm1), plm_r = 2.0f * (vp1 - v0);
+   const float ssign = plm_l + plm_r;
+   const float c0 = fd_l, c1 = b0, c2 = 0.5f * b1, c3 = b2 * (float)(1.0 / 3.0);
+   const float r1s = (root1 >= 0.0f && root1 <= 1.0f) ? c0 + root1 * (c1 + root1 * (c2 + root1 * c3)) : ssign;
+   const float r2s = (root2 >= 0.0f && root2 <= 1.0f) ? c0 + root2 * (c1 + root2 * (c2 + root2 * c3)) : ssign;
+   if (r1s * ssign < 0.0f || r2s * ssign < 0.0f) {
+      const float third = (float)(1.0 / 3.0);
+      if (fabsf(plm_l) <= fabsf(plm_r)) {
+         // collapse to the left edge (eq. 21), then the PLM-slope checks (eqs. 28, 29)
+         fd_l = third * (10.0f * v0 - 2.0f * fv_r - 8.0f * fv_l);
+         fd_r = -10.0f * v0 + 6.0f * fv_r + 4.0f * fv_l;
+         if (ssign * fd_l < 0.0f) {
+            fd_l = 0.0f;
+            fv_r = 5.0f * v0 - 4.0f * fv_l;
+            fd_r = 20.0f * (v0 - fv_l);
+         } else if (ssign * fd_r < 0.0f) {
+            fd_r = 0.0f;
+            fv_l = 0.5f * (5.0f * v0 - 3.0f * fv_r);
+            fd_l = (float)(10.0 / 3.0) * (-v0 + fv_r);
+         }
+      } else {
+         fd_l = 10.0f * v0 - 6.0f * fv_l - 4.0f * fv_r;
+         fd_r = third * (-10.0f * v0 + 2.0f * fv_l + 8.0f * fv_r);
+         if (ssign * fd_l < 0.0f) {
+            fd_l = 0.0f;
+            fv_r = 0.5f * (5.0f * v0 - 3.0f * fv_l);
+            fd_r = (float)(10.0 / 3.0) * (v0 - fv_l);
+         } else if (ssign * fd_r < 0.0f) {
+            fd_r = 0.0f;
+            fv_l = 5.0f * v0 - 4.0f * fv_r;
+            fd_l = 20.0f * (-v0 + fv_r);
+         }
+      }
+   }
+   a[0] = fv_l;
+   a[1] = 0.5f * fd_l;
+   a[2] = 10.0f * v0 - 4.0f * fv_r - 6.0f * fv_l + 0.5f * (fd_r - 3.0f * fd_l);
+   a[3] = -15.0f * v0 + 1.5f * fd_l - fd_r + 7.0f * fv_r + 8.0f * fv_l;
+   a[4] = 6.0f * v0 + 0.5f * (fd_r - fd_l) - 3.0f * (fv_l + fv_r);
+}
+
+// Reconstruction orders of the acceleration remap (the reference's
+// ACC_SEMILAG_PLM / _PPM / _PQM).
+constexpr int RECON_PLM = 1, RECON_PPM = 2, RECON_PQM = 4;
+
+// Integral of the reconstruction from 0 to u (cpu_acc_map.cpp:585-601),
+// Horner form with FMA.
+template <int RECON>
+__device__ __forceinline__ float recon_integral(float u, const float a[5]) {
+   if constexpr (RECON == RECON_PLM) return u * fmaf(u, a[1], a[0]);
+   if constexpr (RECON == RECON_PPM) return u * fmaf(u, fmaf(u, a[2], a[1]), a[0]);
+   return u * fmaf(u, fmaf(u, fmaf(u, fmaf(u, a[4], a[3]), a[2]), a[1]), a[0]);
+}
+
 // ---------------------------------------------------------------------------
 // 96-bit mask helpers
 // ---------------------------------------------------------------------------
@@ -417,11 +532,6 @@ __device__ __forceinline__ int cell_offset(int i, int j, int g) {
 
 constexpr uint32_t NO_BLOCK = 0xffffffffu;  // a block that exists with all-zero data
 
-// Integral of the PPM profile a0 + a1 u + a2 u^2 ... from 0 to u, in the
-// reference's normalisation (cpu_acc_map.cpp:585-590), Horner form with FMA.
-__device__ __forceinline__ float ppm_integral(float u, float a0, float a1, float a2) {
-   return u * fmaf(u, fmaf(u, a2, a1), a0);
-}
 __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
 template <int DIM>
@@ -475,8 +585,8 @@ __device__ __forceinline__ void select_lanes(float lag, int lane, unsigned hmask
    min_lane = vmin ? imin : 0;
 }
 
-template <int DIM, bool EXACT>
-__global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
+template <int DIM, bool EXACT, int RECON>
+__global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) remap_kernel(
    const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
    const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
@@ -593,7 +703,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
                e2 = fa(fm(gf + 2.0f, dk), im);
             }
          }
-         float p2 = 0.0f, p1 = 0.0f;
+         float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // the previous block (zero padding at a column start)
          float cur[4], nxt[4];
          load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
          if (col_e > col_s) {
@@ -601,7 +711,13 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
          } else {
             nxt[0] = nxt[1] = nxt[2] = nxt[3] = 0.0f;
          }
-         float face = h4_face_mode<!EXACT>(p2, p1, cur[0], cur[1]);
+         // raw left face of the column's first cell (and its derivative for PQM)
+         float face = 0.0f, face_d = 0.0f;
+         if constexpr (RECON == RECON_PPM) face = h4_face_mode<!EXACT>(pw[2], pw[3], cur[0], cur[1]);
+         if constexpr (RECON == RECON_PQM) {
+            face = h8_value(pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3]);
+            face_d = h7_derivative(pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3]);
+         }
          for (int kb = col_s; kb <= col_e; ++kb) {
             float nn[4];
             if (kb + 2 <= col_e) {
@@ -609,16 +725,30 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
             } else {
                nn[0] = nn[1] = nn[2] = nn[3] = 0.0f;
             }
-            const float w[8] = {p2, p1, cur[0], cur[1], cur[2], cur[3], nxt[0], nxt[1]};
+            // cell g of the block is w[g + 4]; the stencil reaches 4 cells each way
+            const float w[12] = {pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3],
+                                 nxt[0], nxt[1], nxt[2], nxt[3]};
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
-               const float fr = h4_face_mode<!EXACT>(w[g + 1], w[g + 2], w[g + 3], w[g + 4]);
-               float a0, a1, a2;
-               if constexpr (EXACT)
-                  ppm_coeff(w[g + 1], w[g + 2], w[g + 3], face, fr, threshold, scale, a0, a1, a2);
-               else
-                  ppm_coeff_fused(w[g + 1], w[g + 2], w[g + 3], face, fr, a0, a1, a2);
-               face = fr;
+               float a[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+               if constexpr (RECON == RECON_PPM) {
+                  const float fr = h4_face_mode<!EXACT>(w[g + 3], w[g + 4], w[g + 5], w[g + 6]);
+                  if constexpr (EXACT)
+                     ppm_coeff(w[g + 3], w[g + 4], w[g + 5], face, fr, threshold, scale, a[0], a[1], a[2]);
+                  else
+                     ppm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], face, fr, a[0], a[1], a[2]);
+                  face = fr;
+               } else if constexpr (RECON == RECON_PQM) {
+                  const float fr = h8_value(w[g + 1], w[g + 2], w[g + 3], w[g + 4], w[g + 5], w[g + 6], w[g + 7],
+                                            w[g + 8]);
+                  const float fdr = h7_derivative(w[g + 1], w[g + 2], w[g + 3], w[g + 4], w[g + 5], w[g + 6],
+                                                  w[g + 7], w[g + 8]);
+                  pqm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], face, fr, face_d, fdr, a);
+                  face = fr;
+                  face_d = fdr;
+               } else {
+                  plm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], a);
+               }
                const float v_l = v_r;
                v_r = fa(v_r, dv);
                if (fused) {
@@ -642,9 +772,9 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
                   // e1 lies beyond v_r then so does e2 and D1 = D2 = De
                   const float u1 = (e1 >= v_r) ? 1.0f : (e1 - v_l) * inv_dv;
                   const float u2 = (e2 >= v_r) ? 1.0f : (e2 - v_l) * inv_dv;
-                  const float De = ppm_integral(1.0f, a0, a1, a2);
-                  const float D1 = ppm_integral(u1, a0, a1, a2);
-                  const float D2 = ppm_integral(u2, a0, a1, a2);
+                  const float De = recon_integral<RECON>(1.0f, a);
+                  const float D1 = recon_integral<RECON>(u1, a);
+                  const float D2 = recon_integral<RECON>(u2, a);
                   acc0 += D1;
                   acc1 += D2 - D1;
                   acc2 += De - D2;
@@ -667,7 +797,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
                         x = (x < v_r) ? x : v_r;
                         const float u = __double2float_rn(__dmul_rn((double)fs(x, v_l), i_dv));
                         const float dl = dens_r;
-                        dens_r = fm(u, fa(a0, fm(u, fa(a1, fm(u, a2)))));
+                        if constexpr (EXACT)
+                           dens_r = fm(u, fa(a[0], fm(u, fa(a[1], fm(u, a[2])))));
+                        else
+                           dens_r = recon_integral<RECON>(u, a);
                         float* t = &ring[(gk & (RING_CELLS - 1)) * 16 + lane];
                         *t = fa(*t, fs(dens_r, dl));
                      }
@@ -688,10 +821,9 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
                lb = (nl < lb) ? nl : lb;
             }
             flush_until(lb >> 2);
-            p2 = cur[2];
-            p1 = cur[3];
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
+               pw[g] = cur[g];
                cur[g] = nxt[g];
                nxt[g] = nn[g];
             }
@@ -737,20 +869,27 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
-                         uint8_t* content_out, double content_threshold, bool exact, int grid, cudaStream_t stream) {
-#define VLGPU_REMAP(D, E)                                                                                     \
-   remap_kernel<D, E><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids, \
-                                                          sweep_cells, status, mesh, wall_margin, set_capacity, \
-                                                          content_out, content_threshold)
+                         uint8_t* content_out, double content_threshold, bool exact, int recon, int grid,
+                         cudaStream_t stream) {
+#define VLGPU_REMAP(D, E, R)                                                                                  \
+   remap_kernel<D, E, R><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids, \
+                                                             sweep_cells, status, mesh, wall_margin, set_capacity, \
+                                                             content_out, content_threshold)
+#define VLGPU_REMAP_DIMS(E, R)            \
+   if (dim == 0) VLGPU_REMAP(0, E, R);    \
+   else if (dim == 1) VLGPU_REMAP(1, E, R); \
+   else VLGPU_REMAP(2, E, R);
    if (exact) {
-      if (dim == 0) VLGPU_REMAP(0, true);
-      else if (dim == 1) VLGPU_REMAP(1, true);
-      else VLGPU_REMAP(2, true);
+      if (recon != RECON_PPM) return cudaErrorInvalidValue;  // the exact mode is PPM only
+      VLGPU_REMAP_DIMS(true, RECON_PPM)
+   } else if (recon == RECON_PLM) {
+      VLGPU_REMAP_DIMS(false, RECON_PLM)
+   } else if (recon == RECON_PQM) {
+      VLGPU_REMAP_DIMS(false, RECON_PQM)
    } else {
-      if (dim == 0) VLGPU_REMAP(0, false);
-      else if (dim == 1) VLGPU_REMAP(1, false);
-      else VLGPU_REMAP(2, false);
+      VLGPU_REMAP_DIMS(false, RECON_PPM)
    }
+#undef VLGPU_REMAP_DIMS
 #undef VLGPU_REMAP
    return cudaGetLastError();
 }
@@ -766,7 +905,7 @@ cudaError_t launch_rebase_work(SweepCounters* counters, cudaStream_t stream) {
 
 int remap_blocks_per_sm() {
    int n = 0;
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2, false>, REMAP_THREADS, 0);
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2, false, RECON_PPM>, REMAP_THREADS, 0);
    return n > 0 ? n : 1;
 }
 

@@ -26,7 +26,7 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
-                         uint8_t* content_out, double content_threshold, bool exact, int grid,
+                         uint8_t* content_out, double content_threshold, bool exact, int recon, int grid,
                          cudaStream_t stream);
 int remap_blocks_per_sm();
 struct CellAccelInputs {
@@ -89,6 +89,7 @@ struct vlgpu_batch {
    int sm_count = 0;
    int remap_grid = 0;
    bool exact = false;  // remap arithmetic: false = fused, true = the reference's operation order
+   int recon = 2;       // acceleration reconstruction: 1 PLM, 2 PPM, 4 PQM
    double vmin_d[3], bs_d[3], dv_d[3];
    // data pools and the lists written by sweeps into them
    uint32_t* gids[2] = {nullptr, nullptr};

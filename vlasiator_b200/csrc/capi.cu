@@ -87,7 +87,7 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
       const bool prof = b->profiling && b->prof_used + 2 <= b->prof_events.size();
       if (prof) VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used], b->stream));
       VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
-                            sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->remap_grid,
+                            sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->recon, b->remap_grid,
                             b->stream));
       if (prof) {
          VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used + 1], b->stream));
@@ -104,7 +104,7 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
                                    cap, cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm, c, c + 1,
                                    first_of_step ? 1 : 0, b->stream));
          VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
-                               sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->sm_count,
+                               sweep_cells, b->status, b->mdev, wm, cap, b->content, thr, b->exact, b->recon, b->sm_count,
                                b->stream));
          b->launches += 3;
          b->remap_launches += 1;
@@ -698,8 +698,15 @@ int vlgpu_batch_max_dt(vlgpu_batch* b, double max_rotation_deg, double* r_dt, do
 }
 
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact) {
-   if (!b) return VLGPU_EINVAL;
+   if (!b || (exact && b->recon != VLGPU_RECON_PPM)) return VLGPU_EINVAL;
    b->exact = exact != 0;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_set_reconstruction(vlgpu_batch* b, int order) {
+   if (!b || (order != VLGPU_RECON_PLM && order != VLGPU_RECON_PPM && order != VLGPU_RECON_PQM)) return VLGPU_EINVAL;
+   if (b->exact && order != VLGPU_RECON_PPM) return VLGPU_EINVAL;
+   b->recon = order;
    return VLGPU_OK;
 }
 

@@ -28,7 +28,7 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
-                         uint8_t* content_out, double content_threshold, bool exact, int grid,
+                         uint8_t* content_out, double content_threshold, bool exact, int recon, int grid,
                          cudaStream_t stream);
 int remap_blocks_per_sm();
 
@@ -222,7 +222,7 @@ extern "C" int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* 
                              NA_MAX_BLOCKS, dst_cap, d_sweep, d_status, d_counters, d_stats, mdev, wm, 0, n_cells, 0,
                              s));
    NA_CHECK(launch_remap((int)dimension, d_sets, d_counters, d_perm, data_in, data_out, gids_out, d_sweep, d_status,
-                         mdev, wm, NA_MAX_BLOCKS, d_content, params->min_value, false, setup.remap_grid, s));
+                         mdev, wm, NA_MAX_BLOCKS, d_content, params->min_value, false, 2, setup.remap_grid, s));
 
    SweepCounters h_counters{};
    NA_CHECK(cudaMemcpyAsync(h_slots, d_dst_slots, sizeof(CellSlot) * n_cells, cudaMemcpyDeviceToHost, s));

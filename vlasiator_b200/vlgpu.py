@@ -83,6 +83,7 @@ SIGNATURES = {
     "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
     "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "vlgpu_batch_set_reconstruction": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_set_grid": (ctypes.c_int, [_vp, _u32p, _dp]),
     "vlgpu_translate": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_double]),
     "vlgpu_batch_max_dt": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp]),
@@ -143,7 +144,7 @@ class Batch:
     """A device-resident batch of spatial cells (one population)."""
 
     def __init__(self, mesh: VelocityMesh, n_cells: int, capacity: int, params: CParamsT | None = None,
-                 device: int = 0, exact: bool = False):
+                 device: int = 0, exact: bool = False, recon: str = "ppm"):
         self.lib = load()
         self.mesh = mesh
         self.n_cells = int(n_cells)
@@ -156,7 +157,14 @@ class Batch:
         _check(self.lib.vlgpu_batch_create(ctypes.byref(m), ctypes.byref(self.params), self.n_cells, self.capacity,
                                            device, ctypes.byref(h)), "vlgpu_batch_create")
         self.h = h
+        self.set_reconstruction(recon)
         self.set_exact(exact)
+
+    def set_reconstruction(self, recon: str):
+        """"plm", "ppm" (default) or "pqm": the reference's ACC_SEMILAG_* choice."""
+        order = {"plm": 1, "ppm": 2, "pqm": 4}[recon]
+        _check(self.lib.vlgpu_batch_set_reconstruction(self.h, order), "vlgpu_batch_set_reconstruction")
+        self.recon = recon
 
     def set_exact(self, exact: bool):
         """exact=True: bit-identical to the reference's map_1d; False: fused remap (1e-5 of peak)."""
