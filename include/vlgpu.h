@@ -283,6 +283,22 @@ int vlgpu_batch_set_exact(vlgpu_batch* b, int exact);
 #define VLGPU_RECON_PQM 4
 int vlgpu_batch_set_reconstruction(vlgpu_batch* b, int order);
 
+/* Captures n_steps (2, 4 or 6) consecutive device steps into a CUDA graph kept
+   in the batch's graph slot `slot` (0..7): acceleration steps as
+   vlgpu_accelerate_device does them (kind 0) or full Vlasov steps as
+   vlgpu_vlasov_step_device does them with dt (kind 1, grid batches), with
+   map_orders[q] for step q.  Nothing runs during the capture.  Every step
+   moves the VDF between two buffer sets, so an even number of steps starts
+   and ends on the same set, and the graph can be replayed any number of
+   times while the batch stays in that state.  Capture after at least one
+   step of the same kind (the state a step leaves), with profiling off. */
+int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, const uint32_t* map_orders,
+                        double dt);
+
+/* Launches the graph in `slot` on the batch's stream (asynchronously).
+   VLGPU_EINVAL if the batch is not in the buffer state of the capture. */
+int vlgpu_batch_replay(vlgpu_batch* b, int slot);
+
 /* Synchronises the batch's stream and returns the first error seen. */
 int vlgpu_batch_sync(vlgpu_batch* b);
 

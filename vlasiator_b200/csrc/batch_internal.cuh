@@ -139,6 +139,19 @@ struct vlgpu_batch {
    SweepCell* h_sweep = nullptr;
    CellAccelInputs* h_accel = nullptr;
    cudaEvent_t ev_sweep = nullptr, ev_accel = nullptr;
+   // captured step sequences (vlgpu_batch_capture): the executable graph and
+   // the buffer state it starts and ends in
+   struct GraphSlot {
+      cudaGraphExec_t exec = nullptr;
+      const uint32_t* st_gids = nullptr;
+      const uint32_t* st_src = nullptr;
+      const vlgpu::CellSlot* st_slots = nullptr;
+      int cur = 0;
+      int adj_next = 0;
+      unsigned long long launches = 0;
+      unsigned long long remap_launches = 0;
+   };
+   GraphSlot graphs[8];
    // host-side accounting
    unsigned long long launches = 0;
    unsigned long long remap_launches = 0;
@@ -167,5 +180,6 @@ int geometry_device(vlgpu_batch* b, uint32_t map_order);
 int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell);
 int translate_device(vlgpu_batch* b, uint32_t dim, double dt);
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt);
+int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);
 
 }  // namespace vlgpu_batch_ops

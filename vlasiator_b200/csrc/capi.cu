@@ -42,6 +42,8 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
    cudaFree(b->moments_r);
+   for (auto& g : b->graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
    for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
    cudaFreeHost(b->h_sweep);
    cudaFreeHost(b->h_accel);
@@ -695,6 +697,76 @@ int vlgpu_batch_max_dt(vlgpu_batch* b, double max_rotation_deg, double* r_dt, do
       e = cudaMemcpyAsync(v_dt, d + b->n_cells, sizeof(double) * b->n_cells, cudaMemcpyDeviceToHost, b->stream);
    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
    return cuda_status(e, "vlgpu_batch_max_dt");
+}
+
+int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, const uint32_t* map_orders,
+                        double dt) {
+   if (!b || slot < 0 || slot >= 8 || (kind != 0 && kind != 1) || n_steps == 0 || n_steps % 2 != 0 ||
+       n_steps > 6 || !map_orders || b->profiling)
+      return VLGPU_EINVAL;
+   if (kind == 1 && !b->has_grid) return VLGPU_EINVAL;
+   for (uint32_t q = 0; q < n_steps; ++q)
+      if (map_orders[q] > 2) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   vlgpu_batch::GraphSlot& g = b->graphs[slot];
+   if (g.exec) {
+      VL_CHECK(cudaGraphExecDestroy(g.exec));
+      g.exec = nullptr;
+   }
+   const vlgpu_batch::GraphSlot start{nullptr, b->st_gids, b->st_src, b->st_slots, b->cur, b->adj_next, 0, 0};
+   const bool content_valid = b->content_valid;
+   const unsigned long long l0 = b->launches, r0 = b->remap_launches;
+   VL_CHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+   int st = VLGPU_OK;
+   for (uint32_t q = 0; q < n_steps && st == VLGPU_OK; ++q)
+      st = kind == 0 ? accelerate_device(b, map_orders[q], false) : vlasov_step_device(b, dt, map_orders[q]);
+   cudaGraph_t graph = nullptr;
+   const cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+   // nothing ran: the host's view of the buffers is the one before the capture
+   const bool same_buffers = b->st_gids == start.st_gids && b->st_src == start.st_src &&
+                             b->st_slots == start.st_slots && b->cur == start.cur && b->adj_next == start.adj_next;
+   b->st_gids = start.st_gids;
+   b->st_src = start.st_src;
+   b->st_slots = start.st_slots;
+   b->cur = start.cur;
+   b->adj_next = start.adj_next;
+   b->content_valid = content_valid;
+   const unsigned long long dl = b->launches - l0, dr = b->remap_launches - r0;
+   b->launches = l0;
+   b->remap_launches = r0;
+   if (st != VLGPU_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+   }
+   VL_CHECK(ec);
+   if (!same_buffers) {
+      cudaGraphDestroy(graph);
+      return VLGPU_EINVAL;
+   }
+   cudaGraphExec_t exec = nullptr;
+   const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+   cudaGraphDestroy(graph);
+   VL_CHECK(ei);
+   g = start;
+   g.exec = exec;
+   g.launches = dl;
+   g.remap_launches = dr;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_replay(vlgpu_batch* b, int slot) {
+   if (!b || slot < 0 || slot >= 8 || !b->graphs[slot].exec) return VLGPU_EINVAL;
+   const vlgpu_batch::GraphSlot& g = b->graphs[slot];
+   if (b->st_gids != g.st_gids || b->st_src != g.st_src || b->st_slots != g.st_slots || b->cur != g.cur ||
+       b->adj_next != g.adj_next)
+      return VLGPU_EINVAL;  // the batch is not in the buffer state the graph was captured in
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaGraphLaunch(g.exec, b->stream));
+   b->launches += g.launches;
+   b->remap_launches += g.remap_launches;
+   b->content_valid = false;
+   return VLGPU_OK;
 }
 
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact) {

@@ -84,6 +84,8 @@ SIGNATURES = {
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
     "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_set_reconstruction": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "vlgpu_batch_capture": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, _u32p, ctypes.c_double]),
+    "vlgpu_batch_replay": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_set_grid": (ctypes.c_int, [_vp, _u32p, _dp]),
     "vlgpu_translate": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_double]),
     "vlgpu_batch_max_dt": (ctypes.c_int, [_vp, ctypes.c_double, _dp, _dp]),
@@ -159,6 +161,15 @@ class Batch:
         self.h = h
         self.set_reconstruction(recon)
         self.set_exact(exact)
+
+    def capture(self, slot: int, kind: str, map_orders, dt: float = 0.0):
+        """Captures len(map_orders) (even) device steps, kind "accel" or "vlasov", into graph slot `slot`."""
+        o = np.ascontiguousarray(map_orders, np.uint32)
+        _check(self.lib.vlgpu_batch_capture(self.h, slot, {"accel": 0, "vlasov": 1}[kind], len(o),
+                                            _p(o, ctypes.c_uint32), float(dt)), "vlgpu_batch_capture")
+
+    def replay(self, slot: int):
+        _check(self.lib.vlgpu_batch_replay(self.h, slot), "vlgpu_batch_replay")
 
     def set_reconstruction(self, recon: str):
         """"plm", "ppm" (default) or "pqm": the reference's ACC_SEMILAG_* choice."""
