@@ -605,6 +605,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
    // (double)v >= content_threshold  <=>  v >= the smallest float >= the threshold
    const float content_thr = __double2float_ru(content_threshold);
 
+   // the ring starts empty; every set flushes all its targets, and a flush
+   // zeroes the slots it reads, so the ring is empty again at each set start
+#pragma unroll
+   for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
    for (;;) {
       uint32_t sidx = 0;
       if (lane == 0) sidx = atomicAdd(&counters->work, 1u);
@@ -627,8 +631,6 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
       // Lagrangian cell is wider than half a source cell
       const float inv_dv = (float)i_dv;
       const bool fused = !EXACT && dk > 0.55f * dv;
-#pragma unroll
-      for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
       int next_flush = mask_next_set(cs.tgt_mask, 0);
       uint32_t out_idx = 0;
       bool range_err = false;
@@ -673,11 +675,11 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          // ---- map one column (cpu_acc_map.cpp:395-631) ----
          float v_r = fa(fm((float)(WID * col_s), dv), v_min);
          int gk_r;
-         int max_lane, min_lane;
+         int max_lane = 0, min_lane = 0;
          {
             const float lag = fd(fs(v_r, im), dk);
             gk_r = __float2int_rz(lag);
-            select_lanes(lag, lane, hmask, max_lane, min_lane);
+            if (!fused) select_lanes(lag, lane, hmask, max_lane, min_lane);  // the exact loop's lanes
          }
          const int gk_lo_col = cf * WID, gk_hi_col = (cl + 1) * WID - 1;
          // fused mode: g0 = the lane's first target (edge(g0+1) > v), e1/e2 =
@@ -687,10 +689,14 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          float gf = (float)g0;
          float e1 = fa(fm(gf + 1.0f, dk), im), e2 = fa(fm(gf + 2.0f, dk), im);
          float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+         // highest target the ring can take before its next flush; a target
+         // handed over is never below the flushed ones (the flush bound is
+         // the lowest g0 of the half-warp)
+         int win_hi = (next_flush + RING_BLOCKS) * WID - 1;
          auto evict = [&](float acc, int g) {
             if (acc != 0.0f) {
                const int t = clampi(g, gk_lo_col, gk_hi_col);
-               range_err |= (t < next_flush * WID) | (t >= (next_flush + RING_BLOCKS) * WID);
+               range_err |= t > win_hi;
                float* r = &ring[(t & (RING_CELLS - 1)) * 16 + lane];
                *r += acc;
             }
@@ -755,18 +761,25 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
                   // first target of this source cell: advance past edges <= v_l
                   // (at most two, as dk > 0.55 dv), handing finished targets
                   // to the ring
-#pragma unroll
-                  for (int q = 0; q < 2; ++q) {
-                     if (e1 <= v_l) {
-                        evict(acc0, g0);
-                        acc0 = acc1;
-                        acc1 = acc2;
-                        acc2 = 0.0f;
-                        ++g0;
-                        gf += 1.0f;
-                        e1 = e2;
-                        e2 = fa(fm(gf + 2.0f, dk), im);
-                     }
+                  if (e1 <= v_l) {
+                     evict(acc0, g0);
+                     acc0 = acc1;
+                     acc1 = acc2;
+                     acc2 = 0.0f;
+                     ++g0;
+                     gf += 1.0f;
+                     e1 = e2;
+                     e2 = fa(fm(gf + 2.0f, dk), im);
+                  }
+                  if (e1 <= v_l) {  // a second edge inside the same source cell
+                     evict(acc0, g0);
+                     acc0 = acc1;
+                     acc1 = acc2;
+                     acc2 = 0.0f;
+                     ++g0;
+                     gf += 1.0f;
+                     e1 = e2;
+                     e2 = fa(fm(gf + 2.0f, dk), im);
                   }
                   // integrals up to the two edges inside the source cell; if
                   // e1 lies beyond v_r then so does e2 and D1 = D2 = De
@@ -821,6 +834,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
                lb = (nl < lb) ? nl : lb;
             }
             flush_until(lb >> 2);
+            win_hi = (next_flush + RING_BLOCKS) * WID - 1;
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
                pw[g] = cur[g];
@@ -835,7 +849,13 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          cl = ncl;
       }
       flush_until(1 << 20);
-      if (__any_sync(hmask, range_err) && lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
+      if (__any_sync(hmask, range_err)) {
+         if (lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
+         // deposits past the ring window may have landed in slots no flush
+         // reads: clear the ring so that the next set starts empty
+#pragma unroll
+         for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
+      }
    }
 }
 
