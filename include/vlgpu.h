@@ -210,6 +210,12 @@ int vlgpu_vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);
    the layout of vlgpu_batch_moments (16 doubles per cell). */
 int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16);
 
+/* 0.5 * ("_R" + "_V") of every moment, as calculateInterpolatedVelocityMoments
+   (vlasovsolver/vlasovmover.cpp:587-631) forms the moments the field solver
+   reads; the "_V" set is the last one computed (vlgpu_accelerate,
+   vlgpu_vlasov_step or vlgpu_batch_moments).  Grid batches. */
+int vlgpu_batch_interpolated_moments(vlgpu_batch* b, double* out16);
+
 /* Time-step limits per cell (host arrays of n_cells): r_dt = the r-space
    limit of reduce_vlasov_dt (vlasovsolver/arch_dt.cpp:34-97) from the cell's
    current blocks and the grid's cell sizes; v_dt = the v-space limit of

@@ -685,6 +685,17 @@ int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16) {
    return VLGPU_OK;
 }
 
+int vlgpu_batch_interpolated_moments(vlgpu_batch* b, double* out16) {
+   if (!b || !out16 || !b->moments_r) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   std::vector<double> r((size_t)MOM_COUNT * b->n_cells);
+   VL_CHECK(cudaMemcpyAsync(r.data(), b->moments_r, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, b->stream));
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   for (size_t q = 0; q < r.size(); ++q) out16[q] = 0.5 * (r[q] + out16[q]);
+   return VLGPU_OK;
+}
+
 int vlgpu_batch_max_dt(vlgpu_batch* b, double max_rotation_deg, double* r_dt, double* v_dt) {
    if (!b || !r_dt || !v_dt || !b->has_grid) return VLGPU_EINVAL;
    VL_CHECK(cudaSetDevice(b->device));

@@ -92,6 +92,7 @@ SIGNATURES = {
     "vlgpu_vlasov_step": (ctypes.c_int, [_vp, ctypes.POINTER(CFieldsT), ctypes.c_double, ctypes.c_uint32]),
     "vlgpu_vlasov_step_device": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_uint32]),
     "vlgpu_batch_moments_r": (ctypes.c_int, [_vp, _dp]),
+    "vlgpu_batch_interpolated_moments": (ctypes.c_int, [_vp, _dp]),
     "vlgpu_server_create": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32,
                                            ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
     "vlgpu_server_destroy": (ctypes.c_int, [_vp]),
@@ -322,6 +323,13 @@ class Batch:
     def moments_r(self) -> np.ndarray:
         out = np.zeros((self.n_cells, 16))
         _check(self.lib.vlgpu_batch_moments_r(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_moments_r")
+        return out
+
+    def interpolated_moments(self) -> np.ndarray:
+        """0.5 (R + V) of every moment (calculateInterpolatedVelocityMoments)."""
+        out = np.zeros((self.n_cells, 16))
+        _check(self.lib.vlgpu_batch_interpolated_moments(self.h, _p(out, ctypes.c_double)),
+               "vlgpu_batch_interpolated_moments")
         return out
 
     def max_dt(self, max_rotation_deg: float = 22.0):
