@@ -210,6 +210,21 @@ int vlgpu_vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);
    the layout of vlgpu_batch_moments (16 doubles per cell). */
 int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16);
 
+/* Initial VDF of every cell from a Maxwellian or tri-Maxwellian
+   (MaxwellianPhaseSpaceDensity / TriMaxwellianPhaseSpaceDensity,
+   projects/project.h:45-73) sampled at the cell centres of the blocks around
+   it (Project::setVelocitySpace, projects/project.cpp:239-260), then pruned by
+   the first block adjustment (grid.cpp:289; with the spatial neighbours on a
+   grid).  Replaces the cells' blocks; clears status and adjustment loss.  The
+   species mass is the batch's. */
+typedef struct vlgpu_maxwellian {
+   double n;        /* number density, m^-3 */
+   double T[3];     /* temperatures along the frame's rows, K (equal and an identity frame: isotropic) */
+   double frame[9]; /* rows: the temperature axes (row-major 3x3) */
+   double V[3];     /* bulk velocity, m/s */
+} vlgpu_maxwellian;
+int vlgpu_batch_fill_maxwellian(vlgpu_batch* b, const vlgpu_maxwellian* cells);
+
 /* 0.5 * ("_R" + "_V") of every moment, as calculateInterpolatedVelocityMoments
    (vlasovsolver/vlasovmover.cpp:587-631) forms the moments the field solver
    reads; the "_V" set is the last one computed (vlgpu_accelerate,

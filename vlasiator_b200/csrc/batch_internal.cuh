@@ -53,6 +53,18 @@ cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const Cel
                           const double vmin[3], const double bs[3], const double dv[3], const double dx[3], double q,
                           double m, double max_rotation_deg, double* r_dt, double* v_dt, uint32_t n_cells,
                           cudaStream_t stream);
+struct FillCell {
+   double n;
+   double T[3];
+   double frame[9];
+   double V[3];
+   int lo[3], hi[3];
+   uint32_t row;
+   uint32_t isotropic;
+};
+cudaError_t launch_fill(const FillCell* cells, uint32_t n_cells, const MeshDev& mesh, const double vmin[3],
+                        const double bs[3], const double dv[3], double mass, uint32_t* gids, float* data,
+                        CellSlot* slots, cudaStream_t stream);
 cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
                                cudaStream_t stream);
 struct TransCounters {

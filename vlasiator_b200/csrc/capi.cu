@@ -1,6 +1,8 @@
 // C ABI of libvlgpu.so: device-resident cell batches and the hot-path entry
 // points declared in include/vlgpu.h.  The batch itself and its internal
 // operations are described in batch_internal.cuh.
+#include <cmath>
+
 #include "batch_internal.cuh"
 
 namespace vlgpu_batch_ops {
@@ -682,6 +684,70 @@ int vlgpu_batch_moments_r(vlgpu_batch* b, double* out16) {
    VL_CHECK(cudaMemcpyAsync(out16, b->moments_r, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
                             b->stream));
    VL_CHECK(cudaStreamSynchronize(b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_fill_maxwellian(vlgpu_batch* b, const vlgpu_maxwellian* cells) {
+   if (!b || !cells) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   const double K_B = 1.3806503e-23, PI = 3.14159265358979323846;
+   const double m = b->params.mass, mv = b->params.min_value;
+   std::vector<FillCell> fc(b->n_cells);
+   uint64_t total = 0;
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      const vlgpu_maxwellian& w = cells[c];
+      FillCell& f = fc[c];
+      f.n = w.n;
+      bool identity = true;
+      for (int q = 0; q < 9; ++q) {
+         f.frame[q] = w.frame[q];
+         identity &= w.frame[q] == ((q % 4 == 0) ? 1.0 : 0.0);
+      }
+      for (int d = 0; d < 3; ++d) {
+         f.T[d] = w.T[d];
+         f.V[d] = w.V[d];
+         if (!(w.T[d] > 0.0)) return VLGPU_EINVAL;
+      }
+      f.isotropic = (identity && w.T[0] == w.T[1] && w.T[1] == w.T[2]) ? 1u : 0u;
+      // candidate box: one block beyond the radius where the density can reach
+      // min_value (as the projects' search does)
+      const double Tmax = std::max(w.T[0], std::max(w.T[1], w.T[2]));
+      const double peak = f.isotropic ? w.n * std::pow(m / (2.0 * PI * K_B * Tmax), 1.5)
+                                      : w.n * std::pow(m / (2.0 * PI * K_B), 1.5) / std::sqrt(w.T[0] * w.T[1] * w.T[2]);
+      const double radius = (peak <= mv) ? 0.0 : std::sqrt(2.0 * K_B * Tmax / m * std::log(peak / mv));
+      bool empty = !(w.n > 0.0) || peak <= mv;
+      for (int d = 0; d < 3; ++d) {
+         int lo = (int)std::floor((w.V[d] - radius - b->vmin_d[d]) / b->bs_d[d]) - 1;
+         int hi = (int)std::floor((w.V[d] + radius - b->vmin_d[d]) / b->bs_d[d]) + 1;
+         lo = std::min(std::max(lo, 0), (int)b->mesh.len[d] - 1);
+         hi = std::min(std::max(hi, 0), (int)b->mesh.len[d] - 1);
+         f.lo[d] = lo;
+         f.hi[d] = empty ? lo - 1 : hi;
+      }
+      f.row = (uint32_t)total;
+      if (!empty) total += (uint64_t)(f.hi[0] - f.lo[0] + 1) * (f.hi[1] - f.lo[1] + 1) * (f.hi[2] - f.lo[2] + 1);
+      if (total > b->capacity) return VLGPU_ENOMEM;
+   }
+   FillCell* d_cells = nullptr;
+   VL_CHECK(cudaStreamSynchronize(b->stream));
+   VL_CHECK(cudaMalloc(&d_cells, sizeof(FillCell) * b->n_cells));
+   cudaError_t e = cudaMemcpy(d_cells, fc.data(), sizeof(FillCell) * b->n_cells, cudaMemcpyHostToDevice);
+   if (e == cudaSuccess)
+      e = launch_fill(d_cells, b->n_cells, b->mdev, b->vmin_d, b->bs_d, b->dv_d, m, b->gids[0], b->data[0],
+                      b->slots[0], b->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+   cudaFree(d_cells);
+   VL_CHECK(e);
+   b->launches += 1;
+   const uint32_t used = (uint32_t)total;
+   VL_CHECK(cudaMemcpy(b->rows_used, &used, sizeof(uint32_t), cudaMemcpyHostToDevice));
+   VL_CHECK(cudaMemset(b->status, 0, sizeof(uint32_t) * b->n_cells));
+   set_direct_state(b, 0);
+   b->content_valid = false;
+   // the first block adjustment prunes the candidates (grid.cpp:289)
+   const int st = adjust_device(b);
+   if (st != VLGPU_OK) return st;
+   VL_CHECK(cudaMemsetAsync(b->loss, 0, sizeof(double) * b->n_cells, b->stream));
    return VLGPU_OK;
 }
 

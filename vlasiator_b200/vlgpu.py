@@ -45,6 +45,11 @@ class CParamsT(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class CMaxwellianT(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_double), ("T", ctypes.c_double * 3), ("frame", ctypes.c_double * 9),
+                ("V", ctypes.c_double * 3)]
+
+
 class CFieldsT(ctypes.Structure):
     _fields_ = [("B", ctypes.c_double * 3), ("curl", ctypes.c_double * 3), ("egradpe", ctypes.c_double * 3)]
 
@@ -93,6 +98,7 @@ SIGNATURES = {
     "vlgpu_vlasov_step_device": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_uint32]),
     "vlgpu_batch_moments_r": (ctypes.c_int, [_vp, _dp]),
     "vlgpu_batch_interpolated_moments": (ctypes.c_int, [_vp, _dp]),
+    "vlgpu_batch_fill_maxwellian": (ctypes.c_int, [_vp, ctypes.POINTER(CMaxwellianT)]),
     "vlgpu_server_create": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32,
                                            ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_vp)]),
     "vlgpu_server_destroy": (ctypes.c_int, [_vp]),
@@ -324,6 +330,27 @@ class Batch:
         out = np.zeros((self.n_cells, 16))
         _check(self.lib.vlgpu_batch_moments_r(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_moments_r")
         return out
+
+    def fill_maxwellian(self, n, T, V, frame=None):
+        """Initial VDF of every cell on the device: n (cells), T (cells or cells x 3),
+        V (cells x 3), frame (cells x 3 x 3 rows = temperature axes; identity if None)."""
+        k = self.n_cells
+        n = np.broadcast_to(np.asarray(n, np.float64), (k,))
+        T = np.asarray(T, np.float64)
+        if T.ndim == 0:
+            T = np.full((k, 3), float(T))
+        elif T.ndim == 1:
+            T = np.repeat(T[:, None], 3, axis=1)
+        V = np.broadcast_to(np.asarray(V, np.float64), (k, 3))
+        R = np.broadcast_to(np.eye(3) if frame is None else np.asarray(frame, np.float64), (k, 3, 3))
+        arr = (CMaxwellianT * k)()
+        for c in range(k):
+            arr[c].n = float(n[c])
+            for d in range(3):
+                arr[c].T[d], arr[c].V[d] = float(T[c, d]), float(V[c, d])
+            for q in range(9):
+                arr[c].frame[q] = float(R[c].reshape(9)[q])
+        _check(self.lib.vlgpu_batch_fill_maxwellian(self.h, arr), "vlgpu_batch_fill_maxwellian")
 
     def interpolated_moments(self) -> np.ndarray:
         """0.5 (R + V) of every moment (calculateInterpolatedVelocityMoments)."""
