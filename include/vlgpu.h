@@ -288,7 +288,9 @@ int vlgpu_batch_stats2(vlgpu_batch* b, uint64_t* out);
    distributes each source cell over its target cells with fused
    multiply-adds and at most three targets per source cell: block sets are
    unchanged, values stay within 1e-5 of the cell's peak per step, and mass
-   is conserved as in the exact mode. */
+   is conserved as in the exact mode.  The same switch selects the
+   translation's arithmetic: exact = 1 is bit-identical to trans_map_1d_amr,
+   exact = 0 uses the uniform-width face, single-precision PPM and FMA. */
 int vlgpu_batch_set_exact(vlgpu_batch* b, int exact);
 
 /* Selects the acceleration reconstruction of later sweeps, the reference's

@@ -122,7 +122,10 @@ def test_vlasov_step_matches_oracle(vl, mesh, orc_sp, exact):
     ref, ref_loss, mom_r, mom_v, isect = orc_sp.vlasov_step(mesh, dims, [(c.gids, c.data) for c in cells],
                                                             np.stack([c.B for c in cells]), dt, mo, (DX, DX, DX),
                                                             MASS_PROTON, CHARGE)
-    np.testing.assert_allclose(got["mom_r"][:, [0, 4, 8, 15]], mom_r[:, [0, 4, 8, 15]], rtol=1e-12)
+    # exact mode: the translation is bit-exact, so the "_R" moments agree to
+    # FP64 rounding; fused mode: within the fused translation's tolerance
+    np.testing.assert_allclose(got["mom_r"][:, [0, 4, 8, 15]], mom_r[:, [0, 4, 8, 15]],
+                               rtol=1e-12 if exact else 1e-6)
     np.testing.assert_allclose(got["isect"], isect, rtol=1e-12, atol=1e-9)
     same32 = np.all(got["isect"].astype(np.float32) == isect.astype(np.float32), axis=1)
     nbrs = grid_neighbors(dims)

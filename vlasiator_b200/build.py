@@ -22,6 +22,7 @@ def build(verbose: bool = False, extra=()) -> str:
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(CSRC, "vlgpu_common.cuh"),
                                                        os.path.join(CSRC, "geometry.cuh"),
                                                        os.path.join(CSRC, "batch_internal.cuh"),
+                                                       os.path.join(CSRC, "fused_ppm.cuh"),
                                                        os.path.join(HERE, "..", "include", "vlgpu.h")])
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
         return LIB

@@ -27,6 +27,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "fused_ppm.cuh"
 #include "vlgpu_common.cuh"
 
 namespace vlgpu {
@@ -47,10 +48,6 @@ __device__ __forceinline__ float h4_face(float vm2, float vm1, float v0, float v
    s = fa(s, fm(7.0f, v0));
    s = fs(s, vp1);
    return dmf(1.0 / 12.0, s);
-}
-// The same face in single precision throughout (fused mode).
-__device__ __forceinline__ float h4_face_fused(float vm2, float vm1, float v0, float vp1) {
-   return fmaf(7.0f, vm1 + v0, -(vm2 + vp1)) * (float)(1.0 / 12.0);
 }
 template <bool FUSED>
 __device__ __forceinline__ float h4_face_mode(float vm2, float vm1, float v0, float vp1) {
@@ -99,153 +96,6 @@ __device__ __forceinline__ void ppm_coeff(float vm1, float v0, float vp1, float 
    a0 = fl;
    a1 = fs(fs(fm(3.0f, v0), fm(2.0f, fl)), fr);
    a2 = fs(fa(fl, fr), fm(2.0f, v0));
-}
-
-// The same coefficients in plain single precision (fused mode): the superbee
-// slope as sign(a) * max(min(|a|, 2|b|), min(2|a|, |b|)) when a and b share a
-// sign (equal to maxmod(minmod(a, 2b), minmod(2a, b))), on unscaled values
-// with sign tests instead of products, and contractible arithmetic.
-__device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, float fl, float fr, float& a0,
-                                                float& a1, float& a2) {
-   const float a = vp1 - v0, b = v0 - vm1;
-   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
-   const float aa = fabsf(a), ab = fabsf(b);
-   const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
-   if (sl == 0.0f) {
-      fl = v0;
-      fr = v0;
-   }
-   const float hs = copysignf(0.5f * sl, a);
-   if ((vm1 - fl) * (fl - v0) < 0.0f) fl = v0 - hs;
-   if ((vp1 - fr) * (fr - v0) < 0.0f) fr = v0 + hs;
-   const float one_sixth = (float)(1.0 / 6.0);
-   const float v3 = 3.0f * v0;
-   {
-      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
-      if (d * e > d * d * one_sixth) fl = v3 - 2.0f * fr;
-   }
-   {
-      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
-      if (-d * d * one_sixth > d * e) fr = v3 - 2.0f * fl;
-   }
-   a0 = fl;
-   a1 = v3 - 2.0f * fl - fr;
-   a2 = fl + fr - 2.0f * v0;
-}
-
-// Superbee slope of (l, m, r) on unscaled values: sign(a) * max(min(|a|, 2|b|),
-// min(2|a|, |b|)) when a = r - m and b = m - l share a sign, else 0.
-__device__ __forceinline__ float superbee_fused(float l, float m, float r) {
-   const float a = r - m, b = m - l;
-   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
-   const float aa = fabsf(a), ab = fabsf(b);
-   return same ? copysignf(fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)), a) : 0.0f;
-}
-
-// PLM coefficients (compute_plm_coeff, cpu_1d_plm.hpp:38-49): f = a0 + 2 a1 t.
-__device__ __forceinline__ void plm_coeff_fused(float vm1, float v0, float vp1, float a[5]) {
-   const float d = superbee_fused(vm1, v0, vp1);
-   a[0] = v0 - 0.5f * d;
-   a[1] = 0.5f * d;
-}
-
-// h8 face value and h7 face derivative of the left face of the cell whose
-// stencil is w0..w7 = values k-4 .. k+3 (cpu_face_estimates.hpp:45-79).
-__device__ __forceinline__ float h8_value(float w0, float w1, float w2, float w3, float w4, float w5, float w6,
-                                          float w7) {
-   return (float)(1.0 / 840.0) *
-          (533.0f * (w3 + w4) - 139.0f * (w2 + w5) + 29.0f * (w1 + w6) - 3.0f * (w0 + w7));
-}
-__device__ __forceinline__ float h7_derivative(float w0, float w1, float w2, float w3, float w4, float w5, float w6,
-                                               float w7) {
-   return (float)(1.0 / 5040.0) *
-          (7175.0f * (w4 - w3) - 889.0f * (w5 - w2) + 119.0f * (w6 - w1) - 9.0f * (w7 - w0));
-}
-
-// PQM coefficients (compute_pqm_coeff, cpu_1d_pqm.hpp:157-176) from the raw
-// h8/h7 faces: the extremum / boundedness / slope filters of
-// compute_filtered_face_values_derivatives (cpu_face_estimates.hpp:216-275)
-// and the inflexion-point filter filter_pqm_monotonicity (cpu_1d_pqm.hpp:
-// 31-156), in single precision.
-__device__ __forceinline__ void pqm_coeff_fused(float vm1, float v0, float vp1, float fv_l, float fv_r, float fd_l,
-                                                float fd_r, float a[5]) {
-   const float slope = superbee_fused(vm1, v0, vp1);
-   const float slope_abs = fabsf(slope);
-   const float slope_sign = slope > 0.0f ? 1.0f : -1.0f;
-   if (slope_abs == 0.0f) {
-      fv_r = v0;
-      fv_l = v0;
-      fd_l = 0.0f;
-      fd_r = 0.0f;
-   }
-   if ((vm1 - fv_l) * (fv_l - v0) < 0.0f || slope_sign * fd_l < 0.0f) {
-      fv_l = v0 - slope_sign * 0.5f * slope_abs;
-      fd_l = slope_sign * slope_abs;
-   }
-   if ((vp1 - fv_r) * (fv_r - v0) < 0.0f || slope_sign * fd_r < 0.0f) {
-      fv_r = v0 + slope_sign * 0.5f * slope_abs;
-      fd_r = slope_sign * slope_abs;
-   }
-   // second-derivative coefficients (White and Adcroft 2008, eq. 23)
-   const float b0 = 60.0f * v0 - 24.0f * fv_r - 36.0f * fv_l + 3.0f * (fd_r - 3.0f * fd_l);
-   const float b1 = -360.0f * v0 + 36.0f * fd_l - 24.0f * fd_r + 168.0f * fv_r + 192.0f * fv_l;
-   const float b2 = 360.0f * v0 + 30.0f * (fd_r - fd_l) - 180.0f * (fv_l + fv_r);
-   const float disc = b1 * b1 - 4.0f * b0 * b2;
-   const float sq = disc < 0.0f ? b1 + 200.0f * b2 : sqrtf(disc);
-   const float root1 = (-b1 + sq) / (2.0f * b2);
-   const float root2 = (-b1 - sq) / (2.0f * b2);
-   const float plm_l = 2.0f * (v0 - vm1), plm_r = 2.0f * (vp1 - v0);
-   const float ssign = plm_l + plm_r;
-   const float c0 = fd_l, c1 = b0, c2 = 0.5f * b1, c3 = b2 * (float)(1.0 / 3.0);
-   const float r1s = (root1 >= 0.0f && root1 <= 1.0f) ? c0 + root1 * (c1 + root1 * (c2 + root1 * c3)) : ssign;
-   const float r2s = (root2 >= 0.0f && root2 <= 1.0f) ? c0 + root2 * (c1 + root2 * (c2 + root2 * c3)) : ssign;
-   if (r1s * ssign < 0.0f || r2s * ssign < 0.0f) {
-      const float third = (float)(1.0 / 3.0);
-      if (fabsf(plm_l) <= fabsf(plm_r)) {
-         // collapse to the left edge (eq. 21), then the PLM-slope checks (eqs. 28, 29)
-         fd_l = third * (10.0f * v0 - 2.0f * fv_r - 8.0f * fv_l);
-         fd_r = -10.0f * v0 + 6.0f * fv_r + 4.0f * fv_l;
-         if (ssign * fd_l < 0.0f) {
-            fd_l = 0.0f;
-            fv_r = 5.0f * v0 - 4.0f * fv_l;
-            fd_r = 20.0f * (v0 - fv_l);
-         } else if (ssign * fd_r < 0.0f) {
-            fd_r = 0.0f;
-            fv_l = 0.5f * (5.0f * v0 - 3.0f * fv_r);
-            fd_l = (float)(10.0 / 3.0) * (-v0 + fv_r);
-         }
-      } else {
-         fd_l = 10.0f * v0 - 6.0f * fv_l - 4.0f * fv_r;
-         fd_r = third * (-10.0f * v0 + 2.0f * fv_l + 8.0f * fv_r);
-         if (ssign * fd_l < 0.0f) {
-            fd_l = 0.0f;
-            fv_r = 0.5f * (5.0f * v0 - 3.0f * fv_l);
-            fd_r = (float)(10.0 / 3.0) * (v0 - fv_l);
-         } else if (ssign * fd_r < 0.0f) {
-            fd_r = 0.0f;
-            fv_l = 5.0f * v0 - 4.0f * fv_r;
-            fd_l = 20.0f * (-v0 + fv_r);
-         }
-      }
-   }
-   a[0] = fv_l;
-   a[1] = 0.5f * fd_l;
-   a[2] = 10.0f * v0 - 4.0f * fv_r - 6.0f * fv_l + 0.5f * (fd_r - 3.0f * fd_l);
-   a[3] = -15.0f * v0 + 1.5f * fd_l - fd_r + 7.0f * fv_r + 8.0f * fv_l;
-   a[4] = 6.0f * v0 + 0.5f * (fd_r - fd_l) - 3.0f * (fv_l + fv_r);
-}
-
-// Reconstruction orders of the acceleration remap (the reference's
-// ACC_SEMILAG_PLM / _PPM / _PQM).
-constexpr int RECON_PLM = 1, RECON_PPM = 2, RECON_PQM = 4;
-
-// Integral of the reconstruction from 0 to u (cpu_acc_map.cpp:585-601),
-// Horner form with FMA.
-template <int RECON>
-__device__ __forceinline__ float recon_integral(float u, const float a[5]) {
-   if constexpr (RECON == RECON_PLM) return u * fmaf(u, a[1], a[0]);
-   if constexpr (RECON == RECON_PPM) return u * fmaf(u, fmaf(u, a[2], a[1]), a[0]);
-   return u * fmaf(u, fmaf(u, fmaf(u, fmaf(u, a[4], a[3]), a[2]), a[1]), a[0]);
 }
 
 // ---------------------------------------------------------------------------

@@ -81,8 +81,8 @@ cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int
 cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, const uint32_t* item_pencil,
                                const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
                                const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
-                               float dz, float threshold, int grid, cudaStream_t stream);
-int trans_blocks_per_sm(uint32_t N);
+                               float dz, float threshold, bool exact, int grid, cudaStream_t stream);
+int trans_blocks_per_sm(uint32_t N, bool exact);
 uint32_t union_words(const MeshDev& mesh);
 constexpr int MOM_COUNT = 16;
 constexpr double MU_0 = 1.25663706e-6;  // physicalconstants::MU_0 (common.h:561)

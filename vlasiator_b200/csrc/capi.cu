@@ -216,10 +216,11 @@ int translate_device(vlgpu_batch* b, uint32_t dim, double dt) {
    VL_CHECK(launch_pencil_union(b->st_gids, b->st_slots, (int)dim, b->grid_dims[0], b->grid_dims[1],
                                 b->grid_dims[2], b->mdev, b->item_gid, b->item_pencil, b->trans_rows,
                                 (uint32_t)b->capacity, b->row_cap, b->tcounters, b->status, b->stream));
-   const int grid = b->sm_count * trans_blocks_per_sm(N);
+   const int grid = b->sm_count * trans_blocks_per_sm(N, b->exact);
    VL_CHECK(launch_trans_remap((int)dim, N, b->item_gid, b->item_pencil, b->trans_rows, b->tcounters,
                                (uint32_t)b->capacity, b->st_src, b->data[b->cur], b->data[d], b->gids[d], b->mdev,
-                               (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, grid, b->stream));
+                               (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, b->exact, grid,
+                               b->stream));
    VL_CHECK(cudaMemcpyAsync(b->slots[d], b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToDevice,
                             b->stream));
    VL_CHECK(cudaMemcpyAsync(b->rows_used + d, b->rows_used + b->st_list, sizeof(uint32_t), cudaMemcpyDeviceToDevice,

@@ -24,11 +24,18 @@
 //                         belongs to exactly one item, so the output pool is
 //                         written once per block, without atomics.
 //
-// Arithmetic follows the reference's scalar build operation by operation
-// (round-to-nearest intrinsics, the same double-precision steps), so the
-// result is bit-identical to the reference's trans_map_1d_amr.
+// In the exact mode the arithmetic follows the reference's scalar build
+// operation by operation (round-to-nearest intrinsics, the same
+// double-precision steps), so the result is bit-identical to the reference's
+// trans_map_1d_amr.  The fused mode (the default, as for the acceleration)
+// uses the uniform-width h4 face the nonuniform one reduces to, the
+// single-precision PPM of the acceleration's fused mode, FMA for the
+// outgoing integral, and no h/h ratio for equal cell widths; it computes the
+// faces inside the coefficient pass, so one shared-memory array and one
+// barrier fewer are needed.
 #include <cstdint>
 
+#include "fused_ppm.cuh"
 #include "vlgpu_common.cuh"
 
 namespace vlgpu {
@@ -235,7 +242,7 @@ __global__ void __launch_bounds__(UNION_THREADS) pencil_union_kernel(
 // ---------------------------------------------------------------------------
 // translation remap: persistent CTAs, one item (pencil, block ID) at a time
 // ---------------------------------------------------------------------------
-template <int DIM>
+template <int DIM, bool FUSED>
 __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
    const uint32_t* __restrict__ item_gid, const uint32_t* __restrict__ item_pencil, const uint32_t* __restrict__ rows,
    TransCounters* __restrict__ tc, uint32_t item_cap, const uint32_t* __restrict__ src_index,
@@ -243,9 +250,9 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
    uint32_t N, FaceConsts fc, float dt, float threshold, float scale) {
    extern __shared__ float tsm[];
    const uint32_t NE = N * WID3;
-   float* V = tsm;           // values of the item's blocks, [x][c]
-   float* F = tsm + NE;      // left face of every cell
-   float* NB = tsm + 2 * NE; // outgoing integral (ngbr) of every cell
+   float* V = tsm;                          // values of the item's blocks, [x][c]
+   float* NB = tsm + NE;                    // outgoing integral (ngbr) of every cell
+   float* F = FUSED ? nullptr : tsm + 2 * NE;  // exact mode: left face of every cell
    __shared__ uint32_t s_row[TR_MAX_N];
    __shared__ uint32_t s_pos[TR_MAX_N];  // bit k: some value of plane k of block x is positive
    __shared__ uint32_t s_item;
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          const float cell_vz = __double2float_rn(((double)(sw[2] * WID + k) + 0.5) * (double)dvz + (double)vz_min);
          const float zt = td(tm(cell_vz, dt), fc.h);
          const bool up = zt > 0.0f;
-         s_z1[k] = up ? __double2float_rn(1.0 - (double)zt) : 0.0f;
+         s_z1[k] = up ? (FUSED ? 1.0f - zt : __double2float_rn(1.0 - (double)zt)) : 0.0f;
          s_z2[k] = up ? 1.0f : -zt;
          s_up[k] = up ? 1 : 0;
       }
@@ -303,13 +310,15 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          if (lane == 0 && bits) atomicOr(&s_pos[x], bits);
       }
       __syncthreads();
-      // pass 2: left faces
-      for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
-         const uint32_t x = e >> 6, c = e & 63;
-         const uint32_t xm2 = (x + 2 * N - 2) % N, xm1 = (x + N - 1) % N, xp1 = (x + 1) % N;
-         F[e] = face_nonuniform(fc, V[xm2 * WID3 + c], V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c]);
+      // pass 2 (exact mode): left faces
+      if constexpr (!FUSED) {
+         for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
+            const uint32_t x = e >> 6, c = e & 63;
+            const uint32_t xm2 = (x + 2 * N - 2) % N, xm1 = (x + N - 1) % N, xp1 = (x + 1) % N;
+            F[e] = face_nonuniform(fc, V[xm2 * WID3 + c], V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c]);
+         }
+         __syncthreads();
       }
-      __syncthreads();
       // pass 3: PPM coefficients and the integral leaving each cell, for the
       // planes that are not skipped
       for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
@@ -320,12 +329,20 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          float ngbr = 0.0f;
          if (act) {
             float a0, a1, a2;
-            t_ppm_coeff(V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c], F[e], F[xp1 * WID3 + c], threshold, scale, a0,
-                        a1, a2);
             const float z1 = s_z1[k], z2 = s_z2[k];
-            const float i2 = tm(z2, ta(a0, tm(z2, ta(a1, tm(z2, a2)))));
-            const float i1 = tm(z1, ta(a0, tm(z1, ta(a1, tm(z1, a2)))));
-            ngbr = ts(i2, i1);
+            if constexpr (FUSED) {
+               const float vm2 = V[xm2 * WID3 + c], vm1 = V[xm1 * WID3 + c], v0 = V[e];
+               const float vp1 = V[xp1 * WID3 + c], vp2 = V[xp2 * WID3 + c];
+               ppm_coeff_fused(vm1, v0, vp1, h4_face_fused(vm2, vm1, v0, vp1), h4_face_fused(vm1, v0, vp1, vp2), a0,
+                               a1, a2);
+               ngbr = z2 * fmaf(z2, fmaf(z2, a2, a1), a0) - z1 * fmaf(z1, fmaf(z1, a2, a1), a0);
+            } else {
+               t_ppm_coeff(V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c], F[e], F[xp1 * WID3 + c], threshold, scale,
+                           a0, a1, a2);
+               const float i2 = tm(z2, ta(a0, tm(z2, ta(a1, tm(z2, a2)))));
+               const float i1 = tm(z1, ta(a0, tm(z1, ta(a1, tm(z1, a2)))));
+               ngbr = ts(i2, i1);
+            }
          }
          NB[e] = ngbr;
       }
@@ -344,10 +361,10 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          if (act_self) out = ta(out, ts(V[e], NB[e]));
          if (s_up[k]) {
             const uint32_t act = (s_pos[xm3] | s_pos[xm2] | s_pos[xm1] | s_pos[x] | s_pos[xp1]) >> k & 1u;
-            if (act) out = ta(out, td(tm(NB[xm1 * WID3 + c], fc.h), fc.h));
+            if (act) out = FUSED ? out + NB[xm1 * WID3 + c] : ta(out, td(tm(NB[xm1 * WID3 + c], fc.h), fc.h));
          } else {
             const uint32_t act = (s_pos[xm1] | s_pos[x] | s_pos[xp1] | s_pos[xp2] | s_pos[xp3]) >> k & 1u;
-            if (act) out = ta(out, td(tm(NB[xp1 * WID3 + c], fc.h), fc.h));
+            if (act) out = FUSED ? out + NB[xp1 * WID3 + c] : ta(out, td(tm(NB[xp1 * WID3 + c], fc.h), fc.h));
          }
          dst[(size_t)r * WID3 + c] = out;
          if (c == 0) dst_gids[r] = gid;
@@ -394,30 +411,40 @@ cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int
    return cudaGetLastError();
 }
 
-size_t trans_smem_bytes(uint32_t N) { return sizeof(float) * 3 * (size_t)N * WID3; }
+size_t trans_smem_bytes(uint32_t N, bool exact) { return sizeof(float) * (exact ? 3 : 2) * (size_t)N * WID3; }
 
-int trans_blocks_per_sm(uint32_t N) {
+int trans_blocks_per_sm(uint32_t N, bool exact) {
    int n = 0;
-   cudaFuncSetAttribute(trans_remap_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trans_smem_bytes(N));
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0>, TR_THREADS, trans_smem_bytes(N));
+   const size_t smem = trans_smem_bytes(N, exact);
+   if (exact) {
+      cudaFuncSetAttribute(trans_remap_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0, false>, TR_THREADS, smem);
+   } else {
+      cudaFuncSetAttribute(trans_remap_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0, true>, TR_THREADS, smem);
+   }
    return n > 0 ? n : 1;
 }
 
 cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, const uint32_t* item_pencil,
                                const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
                                const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
-                               float dz, float threshold, int grid, cudaStream_t stream) {
+                               float dz, float threshold, bool exact, int grid, cudaStream_t stream) {
    const FaceConsts fc = face_consts(dz);
    const float scale = (float)(1.0 / (double)threshold);
-   const size_t smem = trans_smem_bytes(N);
+   const size_t smem = trans_smem_bytes(N, exact);
    cudaError_t e = cudaSuccess;
-#define VLGPU_TR(D)                                                                                            \
-   e = cudaFuncSetAttribute(trans_remap_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-   if (e != cudaSuccess) return e;                                                                             \
-   trans_remap_kernel<D><<<grid, TR_THREADS, smem, stream>>>(item_gid, item_pencil, rows, tc, item_cap,         \
-                                                             src_index, src, dst, dst_gids, mesh, N, fc, dt,     \
-                                                             threshold, scale);
-   if (dim == 0) { VLGPU_TR(0) } else if (dim == 1) { VLGPU_TR(1) } else { VLGPU_TR(2) }
+#define VLGPU_TR(D, F)                                                                                            \
+   e = cudaFuncSetAttribute(trans_remap_kernel<D, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+   if (e != cudaSuccess) return e;                                                                                \
+   trans_remap_kernel<D, F><<<grid, TR_THREADS, smem, stream>>>(item_gid, item_pencil, rows, tc, item_cap,         \
+                                                                src_index, src, dst, dst_gids, mesh, N, fc, dt,     \
+                                                                threshold, scale);
+   if (exact) {
+      if (dim == 0) { VLGPU_TR(0, false) } else if (dim == 1) { VLGPU_TR(1, false) } else { VLGPU_TR(2, false) }
+   } else {
+      if (dim == 0) { VLGPU_TR(0, true) } else if (dim == 1) { VLGPU_TR(1, true) } else { VLGPU_TR(2, true) }
+   }
 #undef VLGPU_TR
    return cudaGetLastError();
 }
