@@ -126,7 +126,10 @@ def test_vlasov_step_matches_oracle(vl, mesh, orc_sp, exact):
     # FP64 rounding; fused mode: within the fused translation's tolerance
     np.testing.assert_allclose(got["mom_r"][:, [0, 4, 8, 15]], mom_r[:, [0, 4, 8, 15]],
                                rtol=1e-12 if exact else 1e-6)
-    np.testing.assert_allclose(got["isect"], isect, rtol=1e-12, atol=1e-9)
+    if exact:
+        np.testing.assert_allclose(got["isect"], isect, rtol=1e-12, atol=1e-9)
+    else:  # the pivot comes from the fused translation's moments
+        np.testing.assert_allclose(got["isect"], isect, rtol=1e-6, atol=1e-2)
     same32 = np.all(got["isect"].astype(np.float32) == isect.astype(np.float32), axis=1)
     nbrs = grid_neighbors(dims)
     exact_cells = 0
