@@ -93,14 +93,16 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    const uint8_t* __restrict__ content, const float* __restrict__ data, const int32_t* __restrict__ neighbors,
    uint32_t* __restrict__ out_gids, uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots,
    double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
-   uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3) {
+   uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3, uint32_t n_cells,
+   uint32_t smem_rows, uint32_t* __restrict__ scratch) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
    __shared__ int s_box[8];
    __shared__ uint32_t s_base, s_flags;
    __shared__ double s_loss[ADJ_THREADS / 32];
 
-   const uint32_t cell = blockIdx.x;
+   // persistent CTAs, one cell at a time
+   for (uint32_t cell = blockIdx.x; cell < n_cells; cell += gridDim.x) {
    const CellSlot s = slots[cell];
    const uint32_t L0 = mesh.len[0], L1 = mesh.len[1], L2 = mesh.len[2];
    if (threadIdx.x == 0) {
@@ -157,9 +159,12 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    if (!any) { y0 = 0; y1 = -1; z0 = 0; z1 = -1; }
    const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
    const uint32_t rows = any ? (uint32_t)(ny * nz) : 0u;
-   uint32_t* C = smem;              // 3 * rows
-   uint32_t* H = smem + 3 * rows;   // 3 * rows
-   uint32_t* prefix = smem + 6 * rows;  // rows
+   // the masks live in shared memory when they fit, else in this CTA's slice
+   // of a global scratch array (a full velocity plane of rows)
+   uint32_t* const base = (rows <= smem_rows) ? smem : scratch + (size_t)blockIdx.x * 7 * L1 * L2;
+   uint32_t* C = base;              // 3 * rows
+   uint32_t* H = base + 3 * rows;   // 3 * rows
+   uint32_t* prefix = base + 6 * rows;  // rows
    for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) C[q] = 0;
    __syncthreads();
    // pass 2: content mask rows
@@ -292,23 +297,38 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       if (s_flags) atomicOr(&status[cell], s_flags);
       if (!ok) atomicOr(&counters->overflow, 1u);
    }
+   __syncthreads();  // the next cell reuses the shared state
+   }
 }
 
-size_t adjust_smem_bytes(const MeshDev& mesh) { return sizeof(uint32_t) * 7 * mesh.len[1] * mesh.len[2] + 16; }
+// Rows of (y, z) masks kept in shared memory; a cell whose box has more uses
+// its CTA's global scratch slice.  1600 rows (45 KB) leave room for four CTAs
+// of 512 threads per SM.
+constexpr uint32_t ADJ_SMEM_ROWS = 1600;
+size_t adjust_smem_bytes() { return sizeof(uint32_t) * 7 * ADJ_SMEM_ROWS; }
+size_t adjust_scratch_words(const MeshDev& mesh) { return (size_t)7 * mesh.len[1] * mesh.len[2]; }
+
+int adjust_blocks_per_sm() {
+   int n = 0;
+   cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adjust_smem_bytes());
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjust_kernel, ADJ_THREADS, adjust_smem_bytes());
+   return n > 0 ? n : 1;
+}
 
 cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const CellSlot* slots,
                           const uint8_t* content, const float* data, const int32_t* neighbors, uint32_t* out_gids,
                           uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
-                          uint32_t n_cells, cudaStream_t stream) {
+                          uint32_t n_cells, uint32_t* scratch, int grid, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
-   const size_t smem = adjust_smem_bytes(mesh);
+   const size_t smem = adjust_smem_bytes();
    cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    if (e != cudaSuccess) return e;
-   adjust_kernel<<<n_cells, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
-                                                          out_src, out_slots, loss, status, counters, out_capacity,
-                                                          mesh, min_value, add_width, dv3);
+   const uint32_t g = (uint32_t)grid < n_cells ? (uint32_t)grid : n_cells;
+   adjust_kernel<<<g, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
+                                                    out_src, out_slots, loss, status, counters, out_capacity, mesh,
+                                                    min_value, add_width, dv3, n_cells, ADJ_SMEM_ROWS, scratch);
    return cudaGetLastError();
 }
 

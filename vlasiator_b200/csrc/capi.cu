@@ -43,6 +43,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->tcounters);
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
+   cudaFree(b->adj_scratch);
    cudaFree(b->moments_r);
    for (auto& g : b->graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -149,7 +150,7 @@ int adjust_device(vlgpu_batch* b) {
                           b->data[b->cur], b->neighbors, b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss,
                           b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
-                          (int)b->params.add_width_v, dv3, b->n_cells, b->stream));
+                          (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid, b->stream));
    b->launches += 1;
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
@@ -307,6 +308,7 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
    cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
    b->remap_grid = b->sm_count * remap_blocks_per_sm();
+   b->adj_grid = b->sm_count * adjust_blocks_per_sm();
    const uint64_t cap = block_capacity;
    for (int p = 0; p < 2; ++p) {
       if ((e = cudaMalloc(&b->gids[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "gids");
@@ -335,6 +337,10 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMalloc(&b->counters, sizeof(SweepCounters))) != cudaSuccess) return fail(e, "counters");
    if ((e = cudaMalloc(&b->stats, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMalloc(&b->rows_used, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
+   if ((e = cudaMalloc(&b->adj_scratch, sizeof(uint32_t) * adjust_scratch_words(b->mdev) *
+                                            (size_t)std::min<uint32_t>((uint32_t)b->adj_grid, n_cells))) !=
+       cudaSuccess)
+      return fail(e, "adjust scratch");
    if ((e = cudaMemset(b->rows_used, 0, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMemset(b->stats, 0, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMallocHost(&b->h_sweep, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "pinned");
