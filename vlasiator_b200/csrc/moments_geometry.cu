@@ -63,7 +63,6 @@ __device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, doubl
 
 constexpr int MOM_THREADS = 256;
 constexpr int MOM_GROUPS = MOM_THREADS / 16;  // 16 threads per velocity block
-constexpr int MOM_UNROLL = 4;                 // blocks in flight per thread group
 constexpr int MOM_MAXSUMS = 10;
 
 template <int N>
@@ -128,6 +127,7 @@ __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(
    const double cx0 = 0.5 * dv0 - U0, cx1 = 1.5 * dv0 - U0, cx2 = 2.5 * dv0 - U0, cx3 = 3.5 * dv0 - U0;
    const uint32_t L0 = mesh.len[0], L1 = mesh.len[1];
    Kahan acc[NS];
+   constexpr int MOM_UNROLL = 8;  // blocks in flight per thread group
    for (uint32_t b0 = grp; b0 < s.count; b0 += MOM_GROUPS * MOM_UNROLL) {
       uint32_t g[MOM_UNROLL], idx[MOM_UNROLL];
 #pragma unroll
