@@ -6,7 +6,8 @@
 //
 // A pencil is the line of cells along the sweep dimension through one
 // (transverse) cell position; all cells have width dz and target ratio 1, and
-// the line wraps around periodically.  Two kernels:
+// the line wraps around periodically.  Per sweep, the union kernel and one of
+// the two remap kernels run:
 //
 //   pencil_union_kernel   one CTA per pencil.  The union of the pencil cells'
 //                         block IDs as a bitmap in shared memory; one "item"
@@ -14,25 +15,34 @@
 //                         item, the list position of that block in each cell
 //                         of the pencil (or none).
 //
-//   trans_remap_kernel    persistent CTAs, one item at a time: the item's N
-//                         blocks (64 cells each, zeros where a cell lacks the
-//                         block) are staged in shared memory; left faces,
-//                         PPM coefficients and the outgoing integral of every
-//                         cell follow in three passes, then each existing
-//                         block gets (own value - outgoing) + incoming from
-//                         the upwind neighbour.  Every block of every cell
-//                         belongs to exactly one item, so the output pool is
-//                         written once per block, without atomics.
+//   trans_fused_kernel    (fused mode, the default) one warp per unit of L
+//                         consecutive pencil cells of one item.  Each lane
+//                         owns two of the 64 velocity columns of the block
+//                         (float2 loads: a warp reads a whole block row), keeps
+//                         the L + 6 cells of its window in registers, and walks
+//                         them once: each face, PPM and outgoing integral is
+//                         computed once per cell (plus the window's halo), the
+//                         plane skip comes from warp ballots, and each existing
+//                         block gets (own value - outgoing) + incoming from the
+//                         upwind neighbour, written straight to the output pool.
+//                         No shared memory and no barriers.
+//
+//   trans_remap_kernel    (exact mode) persistent CTAs, one item at a time:
+//                         the item's N blocks (zeros where a cell lacks the
+//                         block) are staged in shared memory; left faces, PPM
+//                         coefficients and the outgoing integral of every cell
+//                         follow in passes separated by barriers.
+//
+// Every block of every cell belongs to exactly one item, so the output pool is
+// written once per block, without atomics.
 //
 // In the exact mode the arithmetic follows the reference's scalar build
 // operation by operation (round-to-nearest intrinsics, the same
 // double-precision steps), so the result is bit-identical to the reference's
-// trans_map_1d_amr.  The fused mode (the default, as for the acceleration)
-// uses the uniform-width h4 face the nonuniform one reduces to, the
-// single-precision PPM of the acceleration's fused mode, FMA for the
-// outgoing integral, and no h/h ratio for equal cell widths; it computes the
-// faces inside the coefficient pass, so one shared-memory array and one
-// barrier fewer are needed.
+// trans_map_1d_amr.  The fused mode uses the uniform-width h4 face the
+// nonuniform one reduces to, the single-precision PPM of the acceleration's
+// fused mode, FMA for the outgoing integral, and no h/h ratio for equal cell
+// widths.
 #include <cstdint>
 
 #include "fused_ppm.cuh"
@@ -240,9 +250,9 @@ __global__ void __launch_bounds__(UNION_THREADS) pencil_union_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// translation remap: persistent CTAs, one item (pencil, block ID) at a time
+// exact translation remap: persistent CTAs, one item (pencil, block ID) at a time
 // ---------------------------------------------------------------------------
-template <int DIM, bool FUSED>
+template <int DIM>
 __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
    const uint32_t* __restrict__ item_gid, const uint32_t* __restrict__ item_pencil, const uint32_t* __restrict__ rows,
    TransCounters* __restrict__ tc, uint32_t item_cap, const uint32_t* __restrict__ src_index,
@@ -252,7 +262,7 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
    const uint32_t NE = N * WID3;
    float* V = tsm;                          // values of the item's blocks, [x][c]
    float* NB = tsm + NE;                    // outgoing integral (ngbr) of every cell
-   float* F = FUSED ? nullptr : tsm + 2 * NE;  // exact mode: left face of every cell
+   float* F = tsm + 2 * NE;                 // left face of every cell
    __shared__ uint32_t s_row[TR_MAX_N];
    __shared__ uint32_t s_pos[TR_MAX_N];  // bit k: some value of plane k of block x is positive
    __shared__ uint32_t s_item;
@@ -286,7 +296,7 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          const float cell_vz = __double2float_rn(((double)(sw[2] * WID + k) + 0.5) * (double)dvz + (double)vz_min);
          const float zt = td(tm(cell_vz, dt), fc.h);
          const bool up = zt > 0.0f;
-         s_z1[k] = up ? (FUSED ? 1.0f - zt : __double2float_rn(1.0 - (double)zt)) : 0.0f;
+         s_z1[k] = up ? __double2float_rn(1.0 - (double)zt) : 0.0f;
          s_z2[k] = up ? 1.0f : -zt;
          s_up[k] = up ? 1 : 0;
       }
@@ -310,15 +320,13 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          if (lane == 0 && bits) atomicOr(&s_pos[x], bits);
       }
       __syncthreads();
-      // pass 2 (exact mode): left faces
-      if constexpr (!FUSED) {
-         for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
-            const uint32_t x = e >> 6, c = e & 63;
-            const uint32_t xm2 = (x + 2 * N - 2) % N, xm1 = (x + N - 1) % N, xp1 = (x + 1) % N;
-            F[e] = face_nonuniform(fc, V[xm2 * WID3 + c], V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c]);
-         }
-         __syncthreads();
+      // pass 2: left faces
+      for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
+         const uint32_t x = e >> 6, c = e & 63;
+         const uint32_t xm2 = (x + 2 * N - 2) % N, xm1 = (x + N - 1) % N, xp1 = (x + 1) % N;
+         F[e] = face_nonuniform(fc, V[xm2 * WID3 + c], V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c]);
       }
+      __syncthreads();
       // pass 3: PPM coefficients and the integral leaving each cell, for the
       // planes that are not skipped
       for (uint32_t e = threadIdx.x; e < NE; e += blockDim.x) {
@@ -330,19 +338,11 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          if (act) {
             float a0, a1, a2;
             const float z1 = s_z1[k], z2 = s_z2[k];
-            if constexpr (FUSED) {
-               const float vm2 = V[xm2 * WID3 + c], vm1 = V[xm1 * WID3 + c], v0 = V[e];
-               const float vp1 = V[xp1 * WID3 + c], vp2 = V[xp2 * WID3 + c];
-               ppm_coeff_fused(vm1, v0, vp1, h4_face_fused(vm2, vm1, v0, vp1), h4_face_fused(vm1, v0, vp1, vp2), a0,
-                               a1, a2);
-               ngbr = z2 * fmaf(z2, fmaf(z2, a2, a1), a0) - z1 * fmaf(z1, fmaf(z1, a2, a1), a0);
-            } else {
-               t_ppm_coeff(V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c], F[e], F[xp1 * WID3 + c], threshold, scale,
-                           a0, a1, a2);
-               const float i2 = tm(z2, ta(a0, tm(z2, ta(a1, tm(z2, a2)))));
-               const float i1 = tm(z1, ta(a0, tm(z1, ta(a1, tm(z1, a2)))));
-               ngbr = ts(i2, i1);
-            }
+            t_ppm_coeff(V[xm1 * WID3 + c], V[e], V[xp1 * WID3 + c], F[e], F[xp1 * WID3 + c], threshold, scale, a0,
+                        a1, a2);
+            const float i2 = tm(z2, ta(a0, tm(z2, ta(a1, tm(z2, a2)))));
+            const float i1 = tm(z1, ta(a0, tm(z1, ta(a1, tm(z1, a2)))));
+            ngbr = ts(i2, i1);
          }
          NB[e] = ngbr;
       }
@@ -361,15 +361,159 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
          if (act_self) out = ta(out, ts(V[e], NB[e]));
          if (s_up[k]) {
             const uint32_t act = (s_pos[xm3] | s_pos[xm2] | s_pos[xm1] | s_pos[x] | s_pos[xp1]) >> k & 1u;
-            if (act) out = FUSED ? out + NB[xm1 * WID3 + c] : ta(out, td(tm(NB[xm1 * WID3 + c], fc.h), fc.h));
+            if (act) out = ta(out, td(tm(NB[xm1 * WID3 + c], fc.h), fc.h));
          } else {
             const uint32_t act = (s_pos[xm1] | s_pos[x] | s_pos[xp1] | s_pos[xp2] | s_pos[xp3]) >> k & 1u;
-            if (act) out = FUSED ? out + NB[xp1 * WID3 + c] : ta(out, td(tm(NB[xp1 * WID3 + c], fc.h), fc.h));
+            if (act) out = ta(out, td(tm(NB[xp1 * WID3 + c], fc.h), fc.h));
          }
          dst[(size_t)r * WID3 + c] = out;
          if (c == 0) dst_gids[r] = gid;
       }
       __syncthreads();
+   }
+}
+
+// ---------------------------------------------------------------------------
+// fused translation remap: one warp per unit (item, L consecutive cells)
+// ---------------------------------------------------------------------------
+constexpr int TF_THREADS = 256;
+
+// Lanes whose columns share the plane (index along the sweep dimension) of
+// this lane's first column; a lane owns columns 2 lane and 2 lane + 1.  For
+// DIM 0 the second column lies in the next plane, with the same lanes.
+template <int DIM>
+__device__ __forceinline__ uint32_t plane_lanes(int lane) {
+   if (DIM == 0) return (lane & 1) ? 0xaaaaaaaau : 0x55555555u;
+   if (DIM == 1) return 0x03030303u << (2 * ((lane >> 1) & 3));
+   return 0xffu << (8 * (lane >> 3));
+}
+template <int DIM>
+__device__ __forceinline__ int lane_plane(int lane) {
+   if (DIM == 0) return 2 * (lane & 1);
+   if (DIM == 1) return (lane >> 1) & 3;
+   return lane >> 3;
+}
+
+// Shift of plane k of the block at swapped index sw2 along the sweep
+// dimension, as fractions of the cell: outgoing integral over [z1, z2]
+// (cpu_trans_map_amr.cpp:60-80; fused arithmetic).
+__device__ __forceinline__ void plane_shift(uint32_t sw2, int k, float dvz, float vz_min, float dt, float h,
+                                            float& z1, float& z2, bool& up) {
+   const float cell_vz = __double2float_rn(((double)(sw2 * WID + k) + 0.5) * (double)dvz + (double)vz_min);
+   const float zt = __fdiv_rn(__fmul_rn(cell_vz, dt), h);
+   up = zt > 0.0f;
+   z1 = up ? 1.0f - zt : 0.0f;
+   z2 = up ? 1.0f : -zt;
+}
+
+// The outgoing integral of one column of window cell j (2 <= j <= W-3) given
+// its left and right faces; zero when the plane is skipped.
+__device__ __forceinline__ float outgoing(float vm1, float v0, float vp1, float fl, float fr, float z1, float z2,
+                                          bool active) {
+   float a0, a1, a2;
+   ppm_coeff_fused(vm1, v0, vp1, fl, fr, a0, a1, a2);
+   const float ngbr = z2 * fmaf(z2, fmaf(z2, a2, a1), a0) - z1 * fmaf(z1, fmaf(z1, a2, a1), a0);
+   return active ? ngbr : 0.0f;
+}
+
+// Unit u covers cells s0 .. s0+L-1 of item u / S (S = ceil(N / L) units per
+// item); its window holds cells s0-3 .. s0+L+2 (periodic), W = L + 6 <= 32, so
+// lane j looks up the list row and data index of window cell j and the warp
+// shares them by shuffles.
+template <int DIM, int L>
+__global__ void __launch_bounds__(TF_THREADS, 3) trans_fused_kernel(
+   const uint32_t* __restrict__ item_gid, const uint32_t* __restrict__ item_pencil, const uint32_t* __restrict__ rows,
+   const TransCounters* __restrict__ tc, uint32_t item_cap, const uint32_t* __restrict__ src_index,
+   const float* __restrict__ src, float* __restrict__ dst, uint32_t* __restrict__ dst_gids, MeshDev mesh,
+   uint32_t N, float dt, float h) {
+   constexpr int W = L + 6;
+   static_assert(W <= 32, "window wider than a warp");
+   constexpr uint32_t FULL = 0xffffffffu;
+   const int lane = threadIdx.x & 31;
+   const uint64_t warp0 = ((uint64_t)blockIdx.x * TF_THREADS + threadIdx.x) >> 5;
+   const uint64_t n_warps = ((uint64_t)gridDim.x * TF_THREADS) >> 5;
+   uint32_t n_items = *((const volatile uint32_t*)&tc->n_items);
+   n_items = (n_items < item_cap) ? n_items : item_cap;
+   const uint32_t S = (N + L - 1) / L;
+   const uint64_t n_units = (uint64_t)n_items * S;
+   const uint32_t pmask = plane_lanes<DIM>(lane);
+   const int kx = lane_plane<DIM>(lane), ky = (DIM == 0) ? kx + 1 : kx;
+   const float dvz = mesh.dv[DIM], vz_min = mesh.vmin[DIM];
+
+   for (uint64_t u = warp0; u < n_units; u += n_warps) {
+      const uint32_t q = (uint32_t)(u / S);
+      const uint32_t s0 = (uint32_t)(u - (uint64_t)q * S) * L;
+      const uint32_t pencil = item_pencil[q];
+      if (pencil == BAD_ITEM) continue;
+      const uint32_t gid = item_gid[q];
+      uint32_t my_row = NO_ROW, my_idx = NO_DATA;
+      if (lane < W) {
+         int t = ((int)s0 - 3 + lane) % (int)N;
+         if (t < 0) t += (int)N;
+         my_row = rows[(uint64_t)q * N + (uint32_t)t];
+         if (my_row != NO_ROW) my_idx = src_index ? src_index[my_row] : my_row;
+      }
+      float2 v[W];
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+         const uint32_t idx = __shfl_sync(FULL, my_idx, j);
+         v[j] = (idx != NO_DATA) ? reinterpret_cast<const float2*>(src + (size_t)idx * WID3)[lane]
+                                 : make_float2(0.0f, 0.0f);
+      }
+      // bit j: the plane of this lane's first (second) column holds a
+      // positive value in window cell j
+      uint32_t posx = 0u, posy = 0u;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+         const uint32_t bx = __ballot_sync(FULL, v[j].x > 0.0f), by = __ballot_sync(FULL, v[j].y > 0.0f);
+         if (DIM == 0) {
+            posx |= (uint32_t)((bx & pmask) != 0u) << j;
+            posy |= (uint32_t)((by & pmask) != 0u) << j;
+         } else {
+            posx |= (uint32_t)(((bx | by) & pmask) != 0u) << j;
+         }
+      }
+      if (DIM != 0) posy = posx;
+      // bit j: some positive value in window cells j-2 .. j+2 (the plane is
+      // remapped for cell j; check_skip_remapping)
+      const uint32_t actx = posx | (posx << 1) | (posx << 2) | (posx >> 1) | (posx >> 2);
+      const uint32_t acty = posy | (posy << 1) | (posy << 2) | (posy >> 1) | (posy >> 2);
+      uint32_t sw[3];
+      swapped_indices(gid, mesh.len, DIM, sw);
+      float z1x, z2x, z1y, z2y;
+      bool upx, upy;
+      plane_shift(sw[2], kx, dvz, vz_min, dt, h, z1x, z2x, upx);
+      plane_shift(sw[2], ky, dvz, vz_min, dt, h, z1y, z2y, upy);
+
+      // walk the window: outgoing integral of cells j = 2 .. W-3, the new
+      // value of cell j-1 as soon as its downwind neighbour's is known
+      float2 fl = make_float2(h4_face_fused(v[0].x, v[1].x, v[2].x, v[3].x),
+                              h4_face_fused(v[0].y, v[1].y, v[2].y, v[3].y));
+      float2 nb_m1 = make_float2(0.0f, 0.0f), nb_0 = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int j = 2; j <= W - 3; ++j) {
+         const float2 fr = make_float2(h4_face_fused(v[j - 1].x, v[j].x, v[j + 1].x, v[j + 2].x),
+                                       h4_face_fused(v[j - 1].y, v[j].y, v[j + 1].y, v[j + 2].y));
+         const float2 nb = make_float2(
+            outgoing(v[j - 1].x, v[j].x, v[j + 1].x, fl.x, fr.x, z1x, z2x, (actx >> j) & 1u),
+            outgoing(v[j - 1].y, v[j].y, v[j + 1].y, fl.y, fr.y, z1y, z2y, (acty >> j) & 1u));
+         fl = fr;
+         const int jo = j - 1;  // output cell, its outgoing is nb_0, upwind nb_m1 / nb
+         if (jo >= 3 && jo <= L + 2) {
+            const uint32_t r = __shfl_sync(FULL, my_row, jo);
+            if (r != NO_ROW && s0 + (uint32_t)(jo - 3) < N) {
+               float2 out;
+               out.x = ((actx >> jo) & 1u) ? v[jo].x - nb_0.x : 0.0f;
+               out.y = ((acty >> jo) & 1u) ? v[jo].y - nb_0.y : 0.0f;
+               out.x = out.x + (upx ? nb_m1.x : nb.x);
+               out.y = out.y + (upy ? nb_m1.y : nb.y);
+               reinterpret_cast<float2*>(dst + (size_t)r * WID3)[lane] = out;
+               if (lane == 0) dst_gids[r] = gid;
+            }
+         }
+         nb_m1 = nb_0;
+         nb_0 = nb;
+      }
    }
 }
 
@@ -411,17 +555,18 @@ cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int
    return cudaGetLastError();
 }
 
-size_t trans_smem_bytes(uint32_t N, bool exact) { return sizeof(float) * (exact ? 3 : 2) * (size_t)N * WID3; }
+size_t trans_smem_bytes(uint32_t N, bool exact) { return exact ? sizeof(float) * 3 * (size_t)N * WID3 : 0; }
 
 int trans_blocks_per_sm(uint32_t N, bool exact) {
    int n = 0;
-   const size_t smem = trans_smem_bytes(N, exact);
    if (exact) {
-      cudaFuncSetAttribute(trans_remap_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0, false>, TR_THREADS, smem);
+      const size_t smem = trans_smem_bytes(N, exact);
+      cudaFuncSetAttribute(trans_remap_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0>, TR_THREADS, smem);
+   } else if (N <= 8) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_fused_kernel<0, 8>, TF_THREADS, 0);
    } else {
-      cudaFuncSetAttribute(trans_remap_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0, true>, TR_THREADS, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_fused_kernel<0, 16>, TF_THREADS, 0);
    }
    return n > 0 ? n : 1;
 }
@@ -430,21 +575,28 @@ cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, co
                                const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
                                const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
                                float dz, float threshold, bool exact, int grid, cudaStream_t stream) {
+   if (!exact) {
+#define VLGPU_TF(D, L)                                                                                      \
+   trans_fused_kernel<D, L><<<grid, TF_THREADS, 0, stream>>>(item_gid, item_pencil, rows, tc, item_cap, src_index, \
+                                                             src, dst, dst_gids, mesh, N, dt, dz);
+      if (N <= 8) {
+         if (dim == 0) { VLGPU_TF(0, 8) } else if (dim == 1) { VLGPU_TF(1, 8) } else { VLGPU_TF(2, 8) }
+      } else {
+         if (dim == 0) { VLGPU_TF(0, 16) } else if (dim == 1) { VLGPU_TF(1, 16) } else { VLGPU_TF(2, 16) }
+      }
+#undef VLGPU_TF
+      return cudaGetLastError();
+   }
    const FaceConsts fc = face_consts(dz);
    const float scale = (float)(1.0 / (double)threshold);
    const size_t smem = trans_smem_bytes(N, exact);
    cudaError_t e = cudaSuccess;
-#define VLGPU_TR(D, F)                                                                                            \
-   e = cudaFuncSetAttribute(trans_remap_kernel<D, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-   if (e != cudaSuccess) return e;                                                                                \
-   trans_remap_kernel<D, F><<<grid, TR_THREADS, smem, stream>>>(item_gid, item_pencil, rows, tc, item_cap,         \
-                                                                src_index, src, dst, dst_gids, mesh, N, fc, dt,     \
-                                                                threshold, scale);
-   if (exact) {
-      if (dim == 0) { VLGPU_TR(0, false) } else if (dim == 1) { VLGPU_TR(1, false) } else { VLGPU_TR(2, false) }
-   } else {
-      if (dim == 0) { VLGPU_TR(0, true) } else if (dim == 1) { VLGPU_TR(1, true) } else { VLGPU_TR(2, true) }
-   }
+#define VLGPU_TR(D)                                                                                              \
+   e = cudaFuncSetAttribute(trans_remap_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+   if (e != cudaSuccess) return e;                                                                               \
+   trans_remap_kernel<D><<<grid, TR_THREADS, smem, stream>>>(item_gid, item_pencil, rows, tc, item_cap, src_index, \
+                                                             src, dst, dst_gids, mesh, N, fc, dt, threshold, scale);
+   if (dim == 0) { VLGPU_TR(0) } else if (dim == 1) { VLGPU_TR(1) } else { VLGPU_TR(2) }
 #undef VLGPU_TR
    return cudaGetLastError();
 }
