@@ -39,6 +39,10 @@ cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, cons
                            double* moments, const MeshDev& mesh, const double vmin[3], const double bs[3],
                            const double dv[3], double mass, double charge, bool second, uint32_t n_cells,
                            cudaStream_t stream);
+cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index, const float* data,
+                                const CellSlot* slots, double* first, double* moments, const MeshDev& mesh,
+                                const double vmin[3], const double bs[3], const double dv[3], double mass,
+                                double charge, uint32_t n_cells, cudaStream_t stream);
 cudaError_t launch_geometry(const CellAccelInputs* in, const double* moments, double* isect12, SweepCell* sweep3,
                             uint32_t n_cells, double q, double m, double hall_min_rhoq, int ohm_gradpe, double mu0,
                             const double vmin[3], const double dv[3], uint32_t map_order, float threshold,
@@ -78,12 +82,13 @@ struct TransCounters {
 constexpr uint32_t TR_MAX_N = 128;
 cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int dim, uint32_t nx, uint32_t ny,
                                 uint32_t nz, const MeshDev& mesh, uint32_t* item_gid, uint32_t* item_pencil,
-                                uint32_t* rows, uint32_t item_cap, uint64_t row_cap, TransCounters* tc,
-                                uint32_t* status, cudaStream_t stream);
+                                uint32_t* rows, uint32_t* srcs, const uint32_t* src_index, uint32_t item_cap,
+                                uint64_t row_cap, TransCounters* tc, uint32_t* status, cudaStream_t stream);
 cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, const uint32_t* item_pencil,
-                               const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
-                               const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
-                               float dz, float threshold, bool exact, int grid, cudaStream_t stream);
+                               const uint32_t* rows, const uint32_t* srcs, TransCounters* tc, uint32_t item_cap,
+                               uint64_t row_cap, const uint32_t* src_index, const float* src, float* dst,
+                               uint32_t* dst_gids, const MeshDev& mesh, float dt, float dz, float threshold, bool exact,
+                               int grid, cudaStream_t stream);
 int trans_blocks_per_sm(uint32_t N, bool exact);
 uint32_t union_words(const MeshDev& mesh);
 constexpr int MOM_COUNT = 16;
@@ -143,7 +148,8 @@ struct vlgpu_batch {
    double grid_dx[3] = {0.0, 0.0, 0.0};
    uint32_t* item_gid = nullptr;
    uint32_t* item_pencil = nullptr;
-   uint32_t* trans_rows = nullptr;
+   uint32_t* trans_rows = nullptr;  // per item and pencil cell: list row of the block (or none)
+   uint32_t* trans_src = nullptr;   // the same entries: data index in the source pool (or none)
    uint64_t row_cap = 0;
    TransCounters* tcounters = nullptr;
    int32_t* neighbors = nullptr;  // 26 per cell (-1: none), the spatial neighbours block adjustment consults
@@ -190,10 +196,11 @@ void free_batch(vlgpu_batch* b);
 void set_direct_state(vlgpu_batch* b, int pool);
 int sweep_device(vlgpu_batch* b, const vlgpu::SweepCell* sweep_cells, uint32_t dim, bool per_cell, bool first_of_step);
 int moments_device(vlgpu_batch* b, bool second, double* record = nullptr);
+int moments_pair_device(vlgpu_batch* b, double* first, double* record);
 int adjust_device(vlgpu_batch* b);
 int materialize(vlgpu_batch* b);
-int geometry_device(vlgpu_batch* b, uint32_t map_order);
-int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell);
+int geometry_device(vlgpu_batch* b, uint32_t map_order, bool have_pivot = false);
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool have_pivot = false);
 int translate_device(vlgpu_batch* b, uint32_t dim, double dt);
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt);
 int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);

@@ -40,6 +40,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->item_gid);
    cudaFree(b->item_pencil);
    cudaFree(b->trans_rows);
+   cudaFree(b->trans_src);
    cudaFree(b->tcounters);
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
@@ -141,6 +142,16 @@ int moments_device(vlgpu_batch* b, bool second, double* record) {
    return VLGPU_OK;
 }
 
+// First moments into `first` (nullptr: into `record`), then the second
+// moments about that bulk velocity into `record`, in one launch.
+int moments_pair_device(vlgpu_batch* b, double* first, double* record) {
+   b->launches += 1;
+   VL_CHECK(launch_moments_pair(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, first, record, b->mdev,
+                                b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, b->n_cells,
+                                b->stream));
+   return VLGPU_OK;
+}
+
 int adjust_device(vlgpu_batch* b) {
    const int a = b->adj_next;
    b->adj_next = 1 - a;
@@ -182,10 +193,13 @@ int materialize(vlgpu_batch* b) {
 }
 
 // Pivot moments and the per-cell FP64 geometry of one acceleration step.
-int geometry_device(vlgpu_batch* b, uint32_t map_order) {
-   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420)
-   int st = moments_device(b, false);
-   if (st != VLGPU_OK) return st;
+int geometry_device(vlgpu_batch* b, uint32_t map_order, bool have_pivot) {
+   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420),
+   // unless the caller has just written the first moments of this VDF
+   if (!have_pivot) {
+      const int st = moments_device(b, false);
+      if (st != VLGPU_OK) return st;
+   }
    b->launches += 1;
    VL_CHECK(launch_geometry(b->accel_in, b->moments, b->isect12, b->sweep3, b->n_cells, b->params.charge,
                             b->params.mass, b->params.hall_minimum_rhoq, (int)b->params.ohm_gradpe, MU_0, b->vmin_d,
@@ -193,8 +207,8 @@ int geometry_device(vlgpu_batch* b, uint32_t map_order) {
    return VLGPU_OK;
 }
 
-int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell) {
-   int st = geometry_device(b, map_order);
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool have_pivot) {
+   int st = geometry_device(b, map_order, have_pivot);
    if (st != VLGPU_OK) return st;
    static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
    for (int s = 0; s < 3; ++s) {
@@ -216,11 +230,12 @@ int translate_device(vlgpu_batch* b, uint32_t dim, double dt) {
    VL_CHECK(cudaMemsetAsync(b->tcounters, 0, sizeof(TransCounters), b->stream));
    VL_CHECK(launch_pencil_union(b->st_gids, b->st_slots, (int)dim, b->grid_dims[0], b->grid_dims[1],
                                 b->grid_dims[2], b->mdev, b->item_gid, b->item_pencil, b->trans_rows,
-                                (uint32_t)b->capacity, b->row_cap, b->tcounters, b->status, b->stream));
+                                b->trans_src, b->st_src, (uint32_t)b->capacity, b->row_cap, b->tcounters, b->status,
+                                b->stream));
    const int grid = b->sm_count * trans_blocks_per_sm(N, b->exact);
-   VL_CHECK(launch_trans_remap((int)dim, N, b->item_gid, b->item_pencil, b->trans_rows, b->tcounters,
-                               (uint32_t)b->capacity, b->st_src, b->data[b->cur], b->data[d], b->gids[d], b->mdev,
-                               (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, b->exact, grid,
+   VL_CHECK(launch_trans_remap((int)dim, N, b->item_gid, b->item_pencil, b->trans_rows, b->trans_src, b->tcounters,
+                               (uint32_t)b->capacity, b->row_cap, b->st_src, b->data[b->cur], b->data[d], b->gids[d],
+                               b->mdev, (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, b->exact, grid,
                                b->stream));
    VL_CHECK(cudaMemcpyAsync(b->slots[d], b->st_slots, sizeof(CellSlot) * b->n_cells, cudaMemcpyDeviceToDevice,
                             b->stream));
@@ -242,10 +257,10 @@ int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order) {
       const int st = translate_device(b, trans_order[s], dt);
       if (st != VLGPU_OK) return st;
    }
-   int st = moments_device(b, false, b->moments_r);
-   if (st == VLGPU_OK) st = moments_device(b, true, b->moments_r);
+   // "_R" moments; their first pass is also the acceleration's pivot record
+   const int st = moments_pair_device(b, b->moments, b->moments_r);
    if (st != VLGPU_OK) return st;
-   return accelerate_device(b, map_order, false);
+   return accelerate_device(b, map_order, false, true);
 }
 
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
@@ -545,10 +560,9 @@ int vlgpu_batch_rho_loss(vlgpu_batch* b, double* out) {
 int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16) {
    if (!b || !out16) return VLGPU_EINVAL;
    VL_CHECK(cudaSetDevice(b->device));
-   // the second-moments pass takes its reference velocity from the record,
-   // so the bulk velocity of the current VDF is computed first
-   int st = moments_device(b, false);
-   if (st == VLGPU_OK && compute_second) st = moments_device(b, true);
+   // the second moments are taken about the bulk velocity of the current VDF,
+   // found by a first pass over each cell in the same launch
+   const int st = compute_second ? moments_pair_device(b, nullptr, b->moments) : moments_device(b, false);
    if (st != VLGPU_OK) return st;
    VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
                             b->stream));
@@ -630,6 +644,7 @@ int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx
       VL_CHECK(cudaMalloc(&b->item_gid, sizeof(uint32_t) * cap));
       VL_CHECK(cudaMalloc(&b->item_pencil, sizeof(uint32_t) * cap));
       VL_CHECK(cudaMalloc(&b->trans_rows, sizeof(uint32_t) * b->row_cap));
+      VL_CHECK(cudaMalloc(&b->trans_src, sizeof(uint32_t) * b->row_cap));
       VL_CHECK(cudaMalloc(&b->tcounters, sizeof(TransCounters)));
       VL_CHECK(cudaMemset(b->tcounters, 0, sizeof(TransCounters)));
    }

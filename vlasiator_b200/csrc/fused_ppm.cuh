@@ -158,4 +158,71 @@ __device__ __forceinline__ float h4_face_fused(float vm2, float vm1, float v0, f
    return fmaf(7.0f, vm1 + v0, -(vm2 + vp1)) * (float)(1.0 / 12.0);
 }
 
+// The same face and PPM for two independent cells at once, with the packed
+// single-precision operations of sm_100 (__fadd2_rn, __fmul2_rn, __ffma2_rn;
+// y - x as fma(x, -1, y), exact before rounding); the limiter's comparisons
+// and selections stay per component.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 p_sub(float2 y, float2 x) { return __ffma2_rn(x, f2(-1.0f), y); }
+
+__device__ __forceinline__ float2 h4_face_x2(float2 vm2, float2 vm1, float2 v0, float2 vp1) {
+   return __ffma2_rn(__fadd2_rn(vm1, v0), f2((float)(7.0 / 12.0)),
+                     __fmul2_rn(__fadd2_rn(vm2, vp1), f2((float)(-1.0 / 12.0))));
+}
+
+// Superbee slope magnitude of one cell (zero at an extremum), the faces
+// flattened to v0 where it is zero, and half the signed slope.
+__device__ __forceinline__ float half_slope(float a, float b, float v0, float& fl, float& fr) {
+   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const float aa = fabsf(a), ab = fabsf(b);
+   const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
+   if (sl == 0.0f) {
+      fl = v0;
+      fr = v0;
+   }
+   return copysignf(0.5f * sl, a);
+}
+
+// ppm_coeff_fused for two cells: f(t) = a0 + a1 t + a2 t^2 on each.
+__device__ __forceinline__ void ppm_coeff_x2(float2 vm1, float2 v0, float2 vp1, float2 fl, float2 fr, float2& a0,
+                                             float2& a1, float2& a2) {
+   const float2 a = p_sub(vp1, v0), b = p_sub(v0, vm1);
+   float2 hs;
+   hs.x = half_slope(a.x, b.x, v0.x, fl.x, fr.x);
+   hs.y = half_slope(a.y, b.y, v0.y, fl.y, fr.y);
+   {
+      const float2 tl = __fmul2_rn(p_sub(vm1, fl), p_sub(fl, v0));
+      const float2 tr = __fmul2_rn(p_sub(vp1, fr), p_sub(fr, v0));
+      const float2 nl = p_sub(v0, hs), nr = __fadd2_rn(v0, hs);
+      if (tl.x < 0.0f) fl.x = nl.x;
+      if (tl.y < 0.0f) fl.y = nl.y;
+      if (tr.x < 0.0f) fr.x = nr.x;
+      if (tr.y < 0.0f) fr.y = nr.y;
+   }
+   const float2 sixth = f2((float)(1.0 / 6.0));
+   const float2 v3 = __fmul2_rn(v0, f2(3.0f));
+   {
+      const float2 d = p_sub(fr, fl), e = __ffma2_rn(__fadd2_rn(fl, fr), f2(-0.5f), v0);
+      const float2 de = __fmul2_rn(d, e), dd = __fmul2_rn(__fmul2_rn(d, d), sixth);
+      const float2 alt = __ffma2_rn(fr, f2(-2.0f), v3);
+      if (de.x > dd.x) fl.x = alt.x;
+      if (de.y > dd.y) fl.y = alt.y;
+   }
+   {
+      const float2 d = p_sub(fr, fl), e = __ffma2_rn(__fadd2_rn(fl, fr), f2(-0.5f), v0);
+      const float2 de = __fmul2_rn(d, e), dd = __fmul2_rn(__fmul2_rn(d, d), sixth);
+      const float2 alt = __ffma2_rn(fl, f2(-2.0f), v3);
+      if (-dd.x > de.x) fr.x = alt.x;
+      if (-dd.y > de.y) fr.y = alt.y;
+   }
+   a0 = fl;
+   a1 = p_sub(__ffma2_rn(fl, f2(-2.0f), v3), fr);
+   a2 = __ffma2_rn(v0, f2(-2.0f), __fadd2_rn(fl, fr));
+}
+
+// Integral of two PPM reconstructions from 0 to u (u * (a0 + u (a1 + u a2))).
+__device__ __forceinline__ float2 ppm_integral_x2(float2 u, float2 a0, float2 a1, float2 a2) {
+   return __fmul2_rn(u, __ffma2_rn(u, __ffma2_rn(u, a2, a1), a0));
+}
+
 }  // namespace vlgpu

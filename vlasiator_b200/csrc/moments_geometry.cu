@@ -108,19 +108,17 @@ __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* s
 // result equals the reference's two-pass sums (first V, then f (v-V)(v-V))
 // up to FP64 rounding.  Without SECOND, U = 0, so the first moments depend
 // on the data alone.
+//
+// moments_pass is one such pass of a CTA over one cell's blocks; thread 0
+// writes the cell's record `out`.
 template <bool SECOND>
-__global__ void __launch_bounds__(MOM_THREADS) moments_kernel(
-   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
-   const CellSlot* __restrict__ slots, double* __restrict__ moments, MeshDev mesh, double vmin0, double vmin1,
-   double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-   double charge) {
+__device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index,
+                                             const float* __restrict__ data, const CellSlot s, double* out,
+                                             const MeshDev& mesh, double vmin0, double vmin1, double vmin2, double bs0,
+                                             double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
+                                             double charge, double U0, double U1, double U2, double* sh_hi,
+                                             double* sh_lo) {
    constexpr int NS = SECOND ? 10 : 4;
-   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   const uint32_t cell = blockIdx.x;
-   const CellSlot s = slots[cell];
-   double* out = moments + (size_t)cell * MOM_COUNT;
-   const double U0 = SECOND ? out[MOM_VX] : 0.0, U1 = SECOND ? out[MOM_VY] : 0.0, U2 = SECOND ? out[MOM_VZ] : 0.0;
    const int sub = threadIdx.x & 15, grp = threadIdx.x >> 4;
    const int j = sub & 3, k = sub >> 2;
    const double cy = (j + 0.5) * dv1 - U1, cz = (k + 0.5) * dv2 - U2;
@@ -207,6 +205,51 @@ __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(
       }
    }
    for (int q = 0; q < 6; ++q) out[MOM_P11 + q] = P[q];
+}
+
+template <bool SECOND>
+__global__ void __launch_bounds__(MOM_THREADS) moments_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
+   const CellSlot* __restrict__ slots, double* __restrict__ moments, MeshDev mesh, double vmin0, double vmin1,
+   double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
+   double charge) {
+   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   const uint32_t cell = blockIdx.x;
+   double* out = moments + (size_t)cell * MOM_COUNT;
+   const double U0 = SECOND ? out[MOM_VX] : 0.0, U1 = SECOND ? out[MOM_VY] : 0.0, U2 = SECOND ? out[MOM_VZ] : 0.0;
+   moments_pass<SECOND>(gids, src_index, data, slots[cell], out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1,
+                        dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo);
+}
+
+// Both passes of a cell in one CTA: the first moments (U = 0) into `first`
+// (or into `moments` when first is null), then the second moments about the
+// bulk velocity just found into `moments`.  The same arithmetic as the
+// first-moments launch followed by the second-moments launch, so the records
+// are identical; the second pass reads the cell's blocks again right after
+// the first, mostly from L2.
+__global__ void __launch_bounds__(MOM_THREADS) moments_pair_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
+   const CellSlot* __restrict__ slots, double* __restrict__ first, double* __restrict__ moments, MeshDev mesh,
+   double vmin0, double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2,
+   double mass, double charge) {
+   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   __shared__ double s_U[3];
+   const uint32_t cell = blockIdx.x;
+   const CellSlot s = slots[cell];
+   double* out = moments + (size_t)cell * MOM_COUNT;
+   double* out1 = first ? first + (size_t)cell * MOM_COUNT : out;
+   moments_pass<false>(gids, src_index, data, s, out1, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
+                       charge, 0.0, 0.0, 0.0, sh_hi, sh_lo);
+   if (threadIdx.x == 0) {
+      s_U[0] = out1[MOM_VX];
+      s_U[1] = out1[MOM_VY];
+      s_U[2] = out1[MOM_VZ];
+   }
+   __syncthreads();
+   moments_pass<true>(gids, src_index, data, s, out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
+                      charge, s_U[0], s_U[1], s_U[2], sh_hi, sh_lo);
 }
 
 // Per-cell acceleration inputs on the device.
@@ -331,6 +374,17 @@ cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, cons
       moments_kernel<false><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, mesh, vmin[0],
                                                                 vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0], dv[1],
                                                                 dv[2], mass, charge);
+   return cudaGetLastError();
+}
+
+cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index, const float* data,
+                                const CellSlot* slots, double* first, double* moments, const MeshDev& mesh,
+                                const double vmin[3], const double bs[3], const double dv[3], double mass,
+                                double charge, uint32_t n_cells, cudaStream_t stream) {
+   if (n_cells == 0) return cudaSuccess;
+   moments_pair_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, first, moments, mesh,
+                                                           vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
+                                                           dv[1], dv[2], mass, charge);
    return cudaGetLastError();
 }
 

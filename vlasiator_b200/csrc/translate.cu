@@ -13,19 +13,23 @@
 //                         block IDs as a bitmap in shared memory; one "item"
 //                         per union block ID (its ID and pencil) and, per
 //                         item, the list position of that block in each cell
-//                         of the pencil (or none).
+//                         of the pencil and its data index in the source pool
+//                         (or none).
 //
-//   trans_fused_kernel    (fused mode, the default) one warp per unit of L
-//                         consecutive pencil cells of one item.  Each lane
-//                         owns two of the 64 velocity columns of the block
-//                         (float2 loads: a warp reads a whole block row), keeps
-//                         the L + 6 cells of its window in registers, and walks
-//                         them once: each face, PPM and outgoing integral is
-//                         computed once per cell (plus the window's halo), the
-//                         plane skip comes from warp ballots, and each existing
-//                         block gets (own value - outgoing) + incoming from the
-//                         upwind neighbour, written straight to the output pool.
-//                         No shared memory and no barriers.
+//   trans_fused_kernel    (fused mode, the default) one warp per item walks
+//                         the whole periodic pencil in batches of 8 cells.
+//                         Each lane owns two of the 64 velocity columns of the
+//                         block (float2 loads: a warp reads a whole block row)
+//                         and keeps a window of 14 cells in registers; each
+//                         face, PPM and outgoing integral is computed once per
+//                         cell (the lane's two columns packed per f32x2
+//                         operation), the
+//                         plane skip comes from warp ballots, and each
+//                         existing block gets (own value - outgoing) + incoming
+//                         from the upwind neighbour, written straight to the
+//                         output pool.  The item's index tables are copied
+//                         into the warp's shared-memory slice with cp.async
+//                         one item ahead; no block-wide barriers.
 //
 //   trans_remap_kernel    (exact mode) persistent CTAs, one item at a time:
 //                         the item's N blocks (zeros where a cell lacks the
@@ -177,8 +181,8 @@ __device__ __forceinline__ uint32_t tr_exclusive_scan(uint32_t v, uint32_t* warp
 __global__ void __launch_bounds__(UNION_THREADS) pencil_union_kernel(
    const uint32_t* __restrict__ gids, const CellSlot* __restrict__ slots, int dim, uint32_t nx, uint32_t ny,
    uint32_t N, uint32_t n_words, uint32_t* __restrict__ item_gid, uint32_t* __restrict__ item_pencil,
-   uint32_t* __restrict__ rows, uint32_t item_cap, uint64_t row_cap, TransCounters* __restrict__ tc,
-   uint32_t* __restrict__ status) {
+   uint32_t* __restrict__ rows, uint32_t* __restrict__ srcs, const uint32_t* __restrict__ src_index,
+   uint32_t item_cap, uint64_t row_cap, TransCounters* __restrict__ tc, uint32_t* __restrict__ status) {
    extern __shared__ uint32_t usm[];
    uint32_t* bm = usm;             // n_words: union bitmap
    uint32_t* pre = usm + n_words;  // n_words: union entries before each word
@@ -236,7 +240,10 @@ __global__ void __launch_bounds__(UNION_THREADS) pencil_union_kernel(
       }
    }
    const uint64_t row0 = (uint64_t)base * N;
-   for (uint64_t e = threadIdx.x; e < (uint64_t)total * N; e += blockDim.x) rows[row0 + e] = NO_ROW;
+   for (uint64_t e = threadIdx.x; e < (uint64_t)total * N; e += blockDim.x) {
+      rows[row0 + e] = NO_ROW;
+      srcs[row0 + e] = NO_DATA;
+   }
    __syncthreads();
    for (uint32_t x = 0; x < N; ++x) {
       const CellSlot s = slots[pencil_cell(p, x, dim, nx, ny)];
@@ -245,6 +252,7 @@ __global__ void __launch_bounds__(UNION_THREADS) pencil_union_kernel(
          const uint32_t w = g >> 5;
          const uint32_t r = pre[w] + __popc(bm[w] & ((1u << (g & 31)) - 1u));
          rows[row0 + (uint64_t)r * N + x] = s.off + b;
+         srcs[row0 + (uint64_t)r * N + x] = src_index ? src_index[s.off + b] : s.off + b;
       }
    }
 }
@@ -377,6 +385,7 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
 // fused translation remap: one warp per unit (item, L consecutive cells)
 // ---------------------------------------------------------------------------
 constexpr int TF_THREADS = 256;
+constexpr int TF_BATCH = 8;  // cells per batch of the walk (16 measured slower)
 
 // Lanes whose columns share the plane (index along the sweep dimension) of
 // this lane's first column; a lane owns columns 2 lane and 2 lane + 1.  For
@@ -416,103 +425,193 @@ __device__ __forceinline__ float outgoing(float vm1, float v0, float vp1, float 
    return active ? ngbr : 0.0f;
 }
 
-// Unit u covers cells s0 .. s0+L-1 of item u / S (S = ceil(N / L) units per
-// item); its window holds cells s0-3 .. s0+L+2 (periodic), W = L + 6 <= 32, so
-// lane j looks up the list row and data index of window cell j and the warp
-// shares them by shuffles.
+// ppm_coeff_fused and the outgoing integral over [z1, z2] for two columns;
+// zero for a column whose plane is skipped.
+__device__ __forceinline__ float2 outgoing_x2(float2 vm1, float2 v0, float2 vp1, float2 fl, float2 fr, float2 z1,
+                                              float2 z2, uint32_t act_x, uint32_t act_y) {
+   float2 a0, a1, a2;
+   ppm_coeff_x2(vm1, v0, vp1, fl, fr, a0, a1, a2);
+   const float2 t2 = __ffma2_rn(z2, __ffma2_rn(z2, a2, a1), a0);
+   const float2 t1 = __ffma2_rn(z1, __ffma2_rn(z1, a2, a1), a0);
+   const float2 ngbr = p_sub(__fmul2_rn(z2, t2), __fmul2_rn(z1, t1));
+   return make_float2(act_x ? ngbr.x : 0.0f, act_y ? ngbr.y : 0.0f);
+}
+
+// This lane's two columns of the block at data index idx (zeros where the
+// cell lacks the block).
+__device__ __forceinline__ float2 load_column_pair(const float* __restrict__ src, uint32_t idx, int lane) {
+   return (idx != NO_DATA) ? reinterpret_cast<const float2*>(src + (size_t)idx * WID3)[lane]
+                           : make_float2(0.0f, 0.0f);
+}
+
+// Bit 0 of the result: the plane of this lane's first (second) column holds
+// a positive value in (x, y).
+template <int DIM>
+__device__ __forceinline__ void plane_positive(float2 v, uint32_t pmask, uint32_t& px, uint32_t& py) {
+   if (DIM == 0) {
+      px = (__ballot_sync(0xffffffffu, v.x > 0.0f) & pmask) != 0u;
+      py = (__ballot_sync(0xffffffffu, v.y > 0.0f) & pmask) != 0u;
+   } else {
+      px = (__ballot_sync(0xffffffffu, (v.x > 0.0f) | (v.y > 0.0f)) & pmask) != 0u;
+      py = px;
+   }
+}
+
+// One warp per item walks the whole (periodic) pencil, L cells per batch.
+// Window index of cell c in the batch that outputs cells s0 .. s0+L-1 is
+// c - s0 + 3; the window holds cells s0-3 .. s0+L+2, the first six carried
+// over from the previous batch.  Carried along the walk: the left face fl of
+// the next cell and the outgoing integrals nb_m1, nb_0 of the two cells before
+// it, so every face and PPM is evaluated once per cell (plus two at the start).
+//
+// The item's header and tables live in the warp's slice of shared memory,
+// double-buffered: [0] pencil, [1] block ID, tsrc[m] (m = 0 .. N+5) = data
+// index of cell (m - 3) mod N (window order, no wrap at use) and trow[x] =
+// list row of output cell x.  The next item's slice is copied in with
+// cp.async while the current item is computed, so only the data loads wait on
+// memory.
+__device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const uint32_t* gmem_src) {
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                "l"(gmem_src)
+                : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+   asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__host__ __device__ constexpr uint32_t tf_slice_words(uint32_t N) { return 2 * N + 8; }
+
 template <int DIM, int L>
 __global__ void __launch_bounds__(TF_THREADS, 3) trans_fused_kernel(
    const uint32_t* __restrict__ item_gid, const uint32_t* __restrict__ item_pencil, const uint32_t* __restrict__ rows,
-   const TransCounters* __restrict__ tc, uint32_t item_cap, const uint32_t* __restrict__ src_index,
+   const uint32_t* __restrict__ srcs, const TransCounters* __restrict__ tc, uint32_t item_cap, uint64_t row_cap,
    const float* __restrict__ src, float* __restrict__ dst, uint32_t* __restrict__ dst_gids, MeshDev mesh,
    uint32_t N, float dt, float h) {
    constexpr int W = L + 6;
-   static_assert(W <= 32, "window wider than a warp");
-   constexpr uint32_t FULL = 0xffffffffu;
+   extern __shared__ uint32_t tf_smem[];
    const int lane = threadIdx.x & 31;
-   const uint64_t warp0 = ((uint64_t)blockIdx.x * TF_THREADS + threadIdx.x) >> 5;
-   const uint64_t n_warps = ((uint64_t)gridDim.x * TF_THREADS) >> 5;
+   uint32_t* const slices = tf_smem + (threadIdx.x >> 5) * 2 * tf_slice_words(N);
+   const uint32_t warp0 = (blockIdx.x * TF_THREADS + threadIdx.x) >> 5;
+   const uint32_t n_warps = (gridDim.x * TF_THREADS) >> 5;
    uint32_t n_items = *((const volatile uint32_t*)&tc->n_items);
    n_items = (n_items < item_cap) ? n_items : item_cap;
-   const uint32_t S = (N + L - 1) / L;
-   const uint64_t n_units = (uint64_t)n_items * S;
    const uint32_t pmask = plane_lanes<DIM>(lane);
    const int kx = lane_plane<DIM>(lane), ky = (DIM == 0) ? kx + 1 : kx;
    const float dvz = mesh.dv[DIM], vz_min = mesh.vmin[DIM];
 
-   for (uint64_t u = warp0; u < n_units; u += n_warps) {
-      const uint32_t q = (uint32_t)(u / S);
-      const uint32_t s0 = (uint32_t)(u - (uint64_t)q * S) * L;
-      const uint32_t pencil = item_pencil[q];
+   // copy item q's header and tables into slice sl (entries past row_cap, of
+   // an item whose pencil did not fit, read as none)
+   auto prefetch = [&](uint32_t q, uint32_t* sl) {
+      if (q >= n_items) {
+         if (lane == 0) sl[0] = BAD_ITEM;
+         return;
+      }
+      if (lane == 0) {
+         cp_async4(sl, item_pencil + q);
+         cp_async4(sl + 1, item_gid + q);
+      }
+      const uint64_t base = (uint64_t)q * N;
+      for (uint32_t m = lane; m < N + 6; m += 32) {
+         const uint32_t cell = (m + 3u * N - 3u) % N;
+         if (base + cell < row_cap) cp_async4(sl + 2 + m, srcs + base + cell);
+         else sl[2 + m] = NO_DATA;
+      }
+      for (uint32_t m = lane; m < N; m += 32) {
+         if (base + m < row_cap) cp_async4(sl + N + 8 + m, rows + base + m);
+         else sl[N + 8 + m] = NO_ROW;
+      }
+      cp_async_commit();
+   };
+
+   prefetch(warp0, slices);
+   uint32_t parity = 0;
+   for (uint32_t q = warp0; q < n_items; q += n_warps, parity ^= 1u) {
+      cp_async_wait_all();
+      __syncwarp();
+      const uint32_t* const sl = slices + parity * tf_slice_words(N);
+      const uint32_t* const tsrc = sl + 2;
+      const uint32_t* const trow = sl + N + 8;
+      const uint32_t pencil = sl[0], gid = sl[1];
+      prefetch(q + n_warps, slices + (parity ^ 1u) * tf_slice_words(N));
       if (pencil == BAD_ITEM) continue;
-      const uint32_t gid = item_gid[q];
-      uint32_t my_row = NO_ROW, my_idx = NO_DATA;
-      if (lane < W) {
-         int t = ((int)s0 - 3 + lane) % (int)N;
-         if (t < 0) t += (int)N;
-         my_row = rows[(uint64_t)q * N + (uint32_t)t];
-         if (my_row != NO_ROW) my_idx = src_index ? src_index[my_row] : my_row;
-      }
-      float2 v[W];
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-         const uint32_t idx = __shfl_sync(FULL, my_idx, j);
-         v[j] = (idx != NO_DATA) ? reinterpret_cast<const float2*>(src + (size_t)idx * WID3)[lane]
-                                 : make_float2(0.0f, 0.0f);
-      }
-      // bit j: the plane of this lane's first (second) column holds a
-      // positive value in window cell j
-      uint32_t posx = 0u, posy = 0u;
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-         const uint32_t bx = __ballot_sync(FULL, v[j].x > 0.0f), by = __ballot_sync(FULL, v[j].y > 0.0f);
-         if (DIM == 0) {
-            posx |= (uint32_t)((bx & pmask) != 0u) << j;
-            posy |= (uint32_t)((by & pmask) != 0u) << j;
-         } else {
-            posx |= (uint32_t)(((bx | by) & pmask) != 0u) << j;
-         }
-      }
-      if (DIM != 0) posy = posx;
-      // bit j: some positive value in window cells j-2 .. j+2 (the plane is
-      // remapped for cell j; check_skip_remapping)
-      const uint32_t actx = posx | (posx << 1) | (posx << 2) | (posx >> 1) | (posx >> 2);
-      const uint32_t acty = posy | (posy << 1) | (posy << 2) | (posy >> 1) | (posy >> 2);
+
       uint32_t sw[3];
       swapped_indices(gid, mesh.len, DIM, sw);
-      float z1x, z2x, z1y, z2y;
+      float2 z1, z2;
       bool upx, upy;
-      plane_shift(sw[2], kx, dvz, vz_min, dt, h, z1x, z2x, upx);
-      plane_shift(sw[2], ky, dvz, vz_min, dt, h, z1y, z2y, upy);
+      plane_shift(sw[2], kx, dvz, vz_min, dt, h, z1.x, z2.x, upx);
+      plane_shift(sw[2], ky, dvz, vz_min, dt, h, z1.y, z2.y, upy);
 
-      // walk the window: outgoing integral of cells j = 2 .. W-3, the new
-      // value of cell j-1 as soon as its downwind neighbour's is known
-      float2 fl = make_float2(h4_face_fused(v[0].x, v[1].x, v[2].x, v[3].x),
-                              h4_face_fused(v[0].y, v[1].y, v[2].y, v[3].y));
-      float2 nb_m1 = make_float2(0.0f, 0.0f), nb_0 = make_float2(0.0f, 0.0f);
+      // window cells -3 .. L+2 of the first batch (past N+2: not needed)
+      float2 w[W];
+      uint32_t posx = 0u, posy = 0u;  // bit j: positive value in window cell j
 #pragma unroll
-      for (int j = 2; j <= W - 3; ++j) {
-         const float2 fr = make_float2(h4_face_fused(v[j - 1].x, v[j].x, v[j + 1].x, v[j + 2].x),
-                                       h4_face_fused(v[j - 1].y, v[j].y, v[j + 1].y, v[j + 2].y));
-         const float2 nb = make_float2(
-            outgoing(v[j - 1].x, v[j].x, v[j + 1].x, fl.x, fr.x, z1x, z2x, (actx >> j) & 1u),
-            outgoing(v[j - 1].y, v[j].y, v[j + 1].y, fl.y, fr.y, z1y, z2y, (acty >> j) & 1u));
-         fl = fr;
-         const int jo = j - 1;  // output cell, its outgoing is nb_0, upwind nb_m1 / nb
-         if (jo >= 3 && jo <= L + 2) {
-            const uint32_t r = __shfl_sync(FULL, my_row, jo);
-            if (r != NO_ROW && s0 + (uint32_t)(jo - 3) < N) {
+      for (int j = 0; j < W; ++j) w[j] = load_column_pair(src, ((uint32_t)j < N + 6) ? tsrc[j] : NO_DATA, lane);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+         uint32_t px, py;
+         plane_positive<DIM>(w[j], pmask, px, py);
+         posx |= px << j;
+         posy |= py << j;
+      }
+      // the outgoing integrals of cells -1 and 0, the left face of cell 1
+      float2 nb_m1, nb_0, fl;
+      {
+         const uint32_t ax = posx | (posx << 1) | (posx << 2) | (posx >> 1) | (posx >> 2);
+         const uint32_t ay = posy | (posy << 1) | (posy << 2) | (posy >> 1) | (posy >> 2);
+         const float2 fm1 = h4_face_x2(w[0], w[1], w[2], w[3]);
+         const float2 f0 = h4_face_x2(w[1], w[2], w[3], w[4]);
+         fl = h4_face_x2(w[2], w[3], w[4], w[5]);
+         nb_m1 = outgoing_x2(w[1], w[2], w[3], fm1, f0, z1, z2, (ax >> 2) & 1u, (ay >> 2) & 1u);
+         nb_0 = outgoing_x2(w[2], w[3], w[4], f0, fl, z1, z2, (ax >> 3) & 1u, (ay >> 3) & 1u);
+      }
+
+      for (uint32_t s0 = 0;;) {
+         // bit j: some positive value in window cells j-2 .. j+2 (the plane is
+         // remapped for that cell; check_skip_remapping)
+         const uint32_t ax = posx | (posx << 1) | (posx << 2) | (posx >> 1) | (posx >> 2);
+         const uint32_t ay = posy | (posy << 1) | (posy << 2) | (posy >> 1) | (posy >> 2);
+#pragma unroll
+         for (int i = 0; i < L; ++i) {
+            // cell y = s0+1+i (window i+4): its right face and outgoing integral;
+            // then the new value of cell y-1 = s0+i (window i+3)
+            const float2 fr = h4_face_x2(w[i + 3], w[i + 4], w[i + 5], w[i + 6]);
+            const float2 nb =
+               outgoing_x2(w[i + 3], w[i + 4], w[i + 5], fl, fr, z1, z2, (ax >> (i + 4)) & 1u, (ay >> (i + 4)) & 1u);
+            fl = fr;
+            const uint32_t r = (s0 + (uint32_t)i < N) ? trow[s0 + i] : NO_ROW;
+            if (r != NO_ROW) {
                float2 out;
-               out.x = ((actx >> jo) & 1u) ? v[jo].x - nb_0.x : 0.0f;
-               out.y = ((acty >> jo) & 1u) ? v[jo].y - nb_0.y : 0.0f;
+               out.x = ((ax >> (i + 3)) & 1u) ? w[i + 3].x - nb_0.x : 0.0f;
+               out.y = ((ay >> (i + 3)) & 1u) ? w[i + 3].y - nb_0.y : 0.0f;
                out.x = out.x + (upx ? nb_m1.x : nb.x);
                out.y = out.y + (upy ? nb_m1.y : nb.y);
                reinterpret_cast<float2*>(dst + (size_t)r * WID3)[lane] = out;
                if (lane == 0) dst_gids[r] = gid;
             }
+            nb_m1 = nb_0;
+            nb_0 = nb;
          }
-         nb_m1 = nb_0;
-         nb_0 = nb;
+         s0 += L;
+         if (s0 >= N) break;
+         // next batch: carry six cells, load cells s0+3 .. s0+L+2
+#pragma unroll
+         for (int j = 0; j < 6; ++j) w[j] = w[L + j];
+         posx >>= L;
+         posy >>= L;
+#pragma unroll
+         for (int j = 0; j < L; ++j) {
+            const uint32_t m = s0 + 6u + (uint32_t)j;
+            w[6 + j] = load_column_pair(src, (m < N + 6) ? tsrc[m] : NO_DATA, lane);
+         }
+#pragma unroll
+         for (int j = 0; j < L; ++j) {
+            uint32_t px, py;
+            plane_positive<DIM>(w[6 + j], pmask, px, py);
+            posx |= px << (6 + j);
+            posy |= py << (6 + j);
+         }
       }
    }
 }
@@ -540,8 +639,8 @@ uint32_t union_words(const MeshDev& mesh) { return (mesh.len[0] * mesh.len[1] * 
 
 cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int dim, uint32_t nx, uint32_t ny,
                                 uint32_t nz, const MeshDev& mesh, uint32_t* item_gid, uint32_t* item_pencil,
-                                uint32_t* rows, uint32_t item_cap, uint64_t row_cap, TransCounters* tc,
-                                uint32_t* status, cudaStream_t stream) {
+                                uint32_t* rows, uint32_t* srcs, const uint32_t* src_index, uint32_t item_cap,
+                                uint64_t row_cap, TransCounters* tc, uint32_t* status, cudaStream_t stream) {
    const uint32_t dims[3] = {nx, ny, nz};
    const uint32_t N = dims[dim];
    const uint32_t n_pencils = nx * ny * nz / N;
@@ -550,12 +649,14 @@ cudaError_t launch_pencil_union(const uint32_t* gids, const CellSlot* slots, int
    cudaError_t e = cudaFuncSetAttribute(pencil_union_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    if (e != cudaSuccess) return e;
    pencil_union_kernel<<<n_pencils, UNION_THREADS, smem, stream>>>(gids, slots, dim, nx, ny, N, n_words, item_gid,
-                                                                     item_pencil, rows, item_cap, row_cap, tc,
-                                                                     status);
+                                                                     item_pencil, rows, srcs, src_index, item_cap,
+                                                                     row_cap, tc, status);
    return cudaGetLastError();
 }
 
 size_t trans_smem_bytes(uint32_t N, bool exact) { return exact ? sizeof(float) * 3 * (size_t)N * WID3 : 0; }
+
+size_t trans_fused_smem_bytes(uint32_t N) { return sizeof(uint32_t) * (TF_THREADS / 32) * 2 * tf_slice_words(N); }
 
 int trans_blocks_per_sm(uint32_t N, bool exact) {
    int n = 0;
@@ -563,27 +664,24 @@ int trans_blocks_per_sm(uint32_t N, bool exact) {
       const size_t smem = trans_smem_bytes(N, exact);
       cudaFuncSetAttribute(trans_remap_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_remap_kernel<0>, TR_THREADS, smem);
-   } else if (N <= 8) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_fused_kernel<0, 8>, TF_THREADS, 0);
    } else {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_fused_kernel<0, 16>, TF_THREADS, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trans_fused_kernel<0, TF_BATCH>, TF_THREADS,
+                                                    trans_fused_smem_bytes(N));
    }
    return n > 0 ? n : 1;
 }
 
 cudaError_t launch_trans_remap(int dim, uint32_t N, const uint32_t* item_gid, const uint32_t* item_pencil,
-                               const uint32_t* rows, TransCounters* tc, uint32_t item_cap, const uint32_t* src_index,
-                               const float* src, float* dst, uint32_t* dst_gids, const MeshDev& mesh, float dt,
-                               float dz, float threshold, bool exact, int grid, cudaStream_t stream) {
+                               const uint32_t* rows, const uint32_t* srcs, TransCounters* tc, uint32_t item_cap,
+                               uint64_t row_cap, const uint32_t* src_index, const float* src, float* dst,
+                               uint32_t* dst_gids, const MeshDev& mesh, float dt, float dz, float threshold, bool exact,
+                               int grid, cudaStream_t stream) {
    if (!exact) {
-#define VLGPU_TF(D, L)                                                                                      \
-   trans_fused_kernel<D, L><<<grid, TF_THREADS, 0, stream>>>(item_gid, item_pencil, rows, tc, item_cap, src_index, \
-                                                             src, dst, dst_gids, mesh, N, dt, dz);
-      if (N <= 8) {
-         if (dim == 0) { VLGPU_TF(0, 8) } else if (dim == 1) { VLGPU_TF(1, 8) } else { VLGPU_TF(2, 8) }
-      } else {
-         if (dim == 0) { VLGPU_TF(0, 16) } else if (dim == 1) { VLGPU_TF(1, 16) } else { VLGPU_TF(2, 16) }
-      }
+      const size_t smem = trans_fused_smem_bytes(N);
+#define VLGPU_TF(D, L)                                                                                    \
+   trans_fused_kernel<D, L><<<grid, TF_THREADS, smem, stream>>>(item_gid, item_pencil, rows, srcs, tc, item_cap, \
+                                                                row_cap, src, dst, dst_gids, mesh, N, dt, dz);
+      if (dim == 0) { VLGPU_TF(0, TF_BATCH) } else if (dim == 1) { VLGPU_TF(1, TF_BATCH) } else { VLGPU_TF(2, TF_BATCH) }
 #undef VLGPU_TF
       return cudaGetLastError();
    }
