@@ -36,9 +36,9 @@ struct CellAccelInputs {
    double dt;
 };
 cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
-                           double* moments, const MeshDev& mesh, const double vmin[3], const double bs[3],
-                           const double dv[3], double mass, double charge, bool second, uint32_t n_cells,
-                           cudaStream_t stream);
+                           double* moments, const double* shift, const MeshDev& mesh, const double vmin[3],
+                           const double bs[3], const double dv[3], double mass, double charge, bool second,
+                           uint32_t n_cells, cudaStream_t stream);
 cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index, const float* data,
                                 const CellSlot* slots, double* first, double* moments, const MeshDev& mesh,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
@@ -130,6 +130,7 @@ struct vlgpu_batch {
    const CellSlot* st_slots = nullptr;
    int cur = 0;                       // data pool holding the values
    bool content_valid = false;        // content[] describes the current list
+   bool pivot_valid = false;          // pivot holds the first moments of the current VDF
    // work arrays
    uint32_t* perm = nullptr;
    ColumnSet* sets = nullptr;
@@ -137,6 +138,7 @@ struct vlgpu_batch {
    SweepCell* sweep3 = nullptr;  // 3 * n_cells, from the device geometry
    CellAccelInputs* accel_in = nullptr;
    double* moments = nullptr;  // MOM_COUNT per cell
+   double* pivot = nullptr;    // MOM_COUNT per cell: first moments (U = 0) the acceleration transform uses
    double* isect12 = nullptr;  // 12 per cell
    double* loss = nullptr;     // RHOLOSSADJUST per cell
    uint32_t* status = nullptr;
@@ -170,6 +172,8 @@ struct vlgpu_batch {
       const vlgpu::CellSlot* st_slots = nullptr;
       int cur = 0;
       int adj_next = 0;
+      bool pivot_valid = false;      // at the start of the captured steps
+      bool pivot_valid_end = false;  // after them
       unsigned long long launches = 0;
       unsigned long long remap_launches = 0;
    };
@@ -195,12 +199,12 @@ int cuda_status(cudaError_t e, const char* what);
 void free_batch(vlgpu_batch* b);
 void set_direct_state(vlgpu_batch* b, int pool);
 int sweep_device(vlgpu_batch* b, const vlgpu::SweepCell* sweep_cells, uint32_t dim, bool per_cell, bool first_of_step);
-int moments_device(vlgpu_batch* b, bool second, double* record = nullptr);
+int moments_device(vlgpu_batch* b, bool second, double* record = nullptr, const double* shift = nullptr);
 int moments_pair_device(vlgpu_batch* b, double* first, double* record);
 int adjust_device(vlgpu_batch* b);
 int materialize(vlgpu_batch* b);
-int geometry_device(vlgpu_batch* b, uint32_t map_order, bool have_pivot = false);
-int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool have_pivot = false);
+int geometry_device(vlgpu_batch* b, uint32_t map_order);
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool next_pivot = true);
 int translate_device(vlgpu_batch* b, uint32_t dim, double dt);
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt);
 int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);

@@ -31,6 +31,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->sweep3);
    cudaFree(b->accel_in);
    cudaFree(b->moments);
+   cudaFree(b->pivot);
    cudaFree(b->isect12);
    cudaFree(b->loss);
    cudaFree(b->status);
@@ -77,6 +78,7 @@ void set_direct_state(vlgpu_batch* b, int pool) {
    b->st_slots = b->slots[pool];
    b->cur = pool;
    b->st_list = pool;
+   b->pivot_valid = false;
 }
 
 // One sweep of every cell; sweep parameters already on the device.
@@ -134,9 +136,9 @@ int run_sweep(vlgpu_batch* b, const double* intersections, size_t stride, uint32
    return sweep_device(b, b->sweep_cells, dim, per_cell, false);
 }
 
-int moments_device(vlgpu_batch* b, bool second, double* record) {
+int moments_device(vlgpu_batch* b, bool second, double* record, const double* shift) {
    b->launches += 1;
-   VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, record ? record : b->moments,
+   VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, record ? record : b->moments, shift,
                            b->mdev, b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, second,
                            b->n_cells, b->stream));
    return VLGPU_OK;
@@ -170,6 +172,7 @@ int adjust_device(vlgpu_batch* b) {
    b->st_slots = b->adj_slots[a];
    b->st_list = 2 + a;
    b->content_valid = false;
+   b->pivot_valid = false;
    return VLGPU_OK;
 }
 
@@ -189,26 +192,29 @@ int materialize(vlgpu_batch* b) {
                             cudaMemcpyDeviceToDevice, b->stream));
    b->st_src = nullptr;
    b->cur = dst;
+   b->pivot_valid = false;
    return VLGPU_OK;
 }
 
 // Pivot moments and the per-cell FP64 geometry of one acceleration step.
-int geometry_device(vlgpu_batch* b, uint32_t map_order, bool have_pivot) {
-   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420),
-   // unless the caller has just written the first moments of this VDF
-   if (!have_pivot) {
-      const int st = moments_device(b, false);
+int geometry_device(vlgpu_batch* b, uint32_t map_order) {
+   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420);
+   // a moments pair that ran on this VDF (the previous step's final moments,
+   // the Vlasov step's "_R" moments) has already written it
+   if (!b->pivot_valid) {
+      const int st = moments_device(b, false, b->pivot);
       if (st != VLGPU_OK) return st;
+      b->pivot_valid = true;
    }
    b->launches += 1;
-   VL_CHECK(launch_geometry(b->accel_in, b->moments, b->isect12, b->sweep3, b->n_cells, b->params.charge,
+   VL_CHECK(launch_geometry(b->accel_in, b->pivot, b->isect12, b->sweep3, b->n_cells, b->params.charge,
                             b->params.mass, b->params.hall_minimum_rhoq, (int)b->params.ohm_gradpe, MU_0, b->vmin_d,
                             b->dv_d, map_order, (float)b->params.min_value, b->stream));
    return VLGPU_OK;
 }
 
-int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool have_pivot) {
-   int st = geometry_device(b, map_order, have_pivot);
+int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool next_pivot) {
+   int st = geometry_device(b, map_order);
    if (st != VLGPU_OK) return st;
    static const uint32_t orders[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
    for (int s = 0; s < 3; ++s) {
@@ -219,7 +225,14 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool ha
    // final block adjustment and moments (vlasovmover.cpp:564-569)
    st = adjust_device(b);
    if (st != VLGPU_OK) return st;
-   return moments_device(b, true);
+   // the "_V" moments: with next_pivot, in one launch with the first moments
+   // of the new VDF as the next step's pivot; else one pass about the pivot
+   // velocity of this step
+   if (!next_pivot) return moments_device(b, true, b->moments, b->pivot);
+   st = moments_pair_device(b, b->pivot, b->moments);
+   if (st != VLGPU_OK) return st;
+   b->pivot_valid = true;
+   return VLGPU_OK;
 }
 
 // One translation sweep of the whole grid along `dim` (trans_map_1d_amr):
@@ -258,9 +271,11 @@ int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order) {
       if (st != VLGPU_OK) return st;
    }
    // "_R" moments; their first pass is also the acceleration's pivot record
-   const int st = moments_pair_device(b, b->moments, b->moments_r);
+   const int st = moments_pair_device(b, b->pivot, b->moments_r);
    if (st != VLGPU_OK) return st;
-   return accelerate_device(b, map_order, false, true);
+   b->pivot_valid = true;
+   // the next step starts with a translation, so its pivot is found anew
+   return accelerate_device(b, map_order, false, false);
 }
 
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt) {
@@ -343,6 +358,8 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMemset(b->accel_in, 0, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "accel");
    if ((e = cudaMalloc(&b->moments, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMemset(b->moments, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMalloc(&b->pivot, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMemset(b->pivot, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMalloc(&b->isect12, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
    if ((e = cudaMemset(b->isect12, 0, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
    if ((e = cudaMalloc(&b->loss, sizeof(double) * n_cells)) != cudaSuccess) return fail(e, "loss");
@@ -562,8 +579,9 @@ int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16) {
    VL_CHECK(cudaSetDevice(b->device));
    // the second moments are taken about the bulk velocity of the current VDF,
    // found by a first pass over each cell in the same launch
-   const int st = compute_second ? moments_pair_device(b, nullptr, b->moments) : moments_device(b, false);
+   const int st = compute_second ? moments_pair_device(b, b->pivot, b->moments) : moments_device(b, false);
    if (st != VLGPU_OK) return st;
+   if (compute_second) b->pivot_valid = true;
    VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
                             b->stream));
    VL_CHECK(cudaStreamSynchronize(b->stream));
@@ -813,7 +831,8 @@ int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, co
       VL_CHECK(cudaGraphExecDestroy(g.exec));
       g.exec = nullptr;
    }
-   const vlgpu_batch::GraphSlot start{nullptr, b->st_gids, b->st_src, b->st_slots, b->cur, b->adj_next, 0, 0};
+   const vlgpu_batch::GraphSlot start{nullptr,      b->st_gids,     b->st_src, b->st_slots, b->cur,
+                                      b->adj_next,  b->pivot_valid, false,     0,           0};
    const bool content_valid = b->content_valid;
    const unsigned long long l0 = b->launches, r0 = b->remap_launches;
    VL_CHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
@@ -831,6 +850,8 @@ int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, co
    b->cur = start.cur;
    b->adj_next = start.adj_next;
    b->content_valid = content_valid;
+   const bool pivot_end = b->pivot_valid;
+   b->pivot_valid = start.pivot_valid;
    const unsigned long long dl = b->launches - l0, dr = b->remap_launches - r0;
    b->launches = l0;
    b->remap_launches = r0;
@@ -849,6 +870,7 @@ int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, co
    VL_CHECK(ei);
    g = start;
    g.exec = exec;
+   g.pivot_valid_end = pivot_end;
    g.launches = dl;
    g.remap_launches = dr;
    return VLGPU_OK;
@@ -858,13 +880,14 @@ int vlgpu_batch_replay(vlgpu_batch* b, int slot) {
    if (!b || slot < 0 || slot >= 8 || !b->graphs[slot].exec) return VLGPU_EINVAL;
    const vlgpu_batch::GraphSlot& g = b->graphs[slot];
    if (b->st_gids != g.st_gids || b->st_src != g.st_src || b->st_slots != g.st_slots || b->cur != g.cur ||
-       b->adj_next != g.adj_next)
-      return VLGPU_EINVAL;  // the batch is not in the buffer state the graph was captured in
+       b->adj_next != g.adj_next || (g.pivot_valid && !b->pivot_valid))
+      return VLGPU_EINVAL;  // the batch is not in the state the graph was captured in
    VL_CHECK(cudaSetDevice(b->device));
    VL_CHECK(cudaGraphLaunch(g.exec, b->stream));
    b->launches += g.launches;
    b->remap_launches += g.remap_launches;
    b->content_valid = false;
+   b->pivot_valid = g.pivot_valid_end;
    return VLGPU_OK;
 }
 

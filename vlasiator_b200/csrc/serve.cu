@@ -239,6 +239,7 @@ int vlgpu_server_tick(vlgpu_server* s, uint32_t* n_active, uint32_t* n_pending, 
       if (b->st_src) rows[b->cur] = (uint32_t)D;
       VL_CHECK(cudaMemcpyAsync(b->rows_used, rows, sizeof(rows), cudaMemcpyHostToDevice, b->stream));
       b->content_valid = false;
+      b->pivot_valid = false;
    }
    for (uint32_t c : admitted) {
       // a new request starts with a clean status word and loss counter
