@@ -16,6 +16,12 @@
 // is a new block list sorted by global ID plus, per block, the index of its
 // data in the current pool (or none for an added block): no VDF value is
 // copied, the next sweep reads the kept blocks where they are.
+//
+// On a grid, content_mask_kernel first writes every cell's content mask once
+// (its content bounding box and the x-mask rows over it, in a pool), so that
+// a cell ORs its 26 neighbours' mask rows instead of walking their block
+// lists; a cell whose mask did not fit (box too large, pool full) is read from
+// its list as before.
 #include <cstdint>
 
 #include "vlgpu_common.cuh"
@@ -88,18 +94,89 @@ __device__ __forceinline__ bool list_block_content(const uint32_t* __restrict__ 
    return block_has_content(data + (size_t)idx * WID3, min_value);
 }
 
+constexpr uint32_t NO_MASK = 0xffffffffu;
+constexpr int MASK_THREADS = 256;
+constexpr uint32_t MASK_SMEM_ROWS = 1600;
+
+// One CTA per cell: the content bounding box (y, z) and, when its rows fit,
+// the content x-mask rows, copied to the pool at an offset taken from
+// pool_top.
+__global__ void __launch_bounds__(MASK_THREADS) content_mask_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
+   const uint8_t* __restrict__ content, const float* __restrict__ data, MeshDev mesh, double min_value,
+   MaskRec* __restrict__ recs, uint32_t* __restrict__ pool, uint32_t* __restrict__ pool_top, uint32_t pool_cap) {
+   __shared__ uint32_t C[3 * MASK_SMEM_ROWS];
+   __shared__ int s_box[4];
+   __shared__ uint32_t s_off;
+   const uint32_t cell = blockIdx.x;
+   const CellSlot s = slots[cell];
+   const uint32_t L0 = mesh.len[0], L1 = mesh.len[1];
+   if (threadIdx.x == 0) {
+      s_box[0] = 1 << 20;
+      s_box[1] = -1;
+      s_box[2] = 1 << 20;
+      s_box[3] = -1;
+   }
+   __syncthreads();
+   {
+      int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
+      for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+         if (list_block_content(src_index, content, data, s.off + b, min_value)) {
+            const uint32_t g = gids[s.off + b];
+            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+            y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
+         }
+      }
+      atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
+      atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
+   }
+   __syncthreads();
+   const int y0 = s_box[0], y1 = s_box[1], z0 = s_box[2], z1 = s_box[3];
+   const int ny = (y1 >= 0) ? y1 - y0 + 1 : 0, nz = (y1 >= 0) ? z1 - z0 + 1 : 0;
+   const uint32_t rows = (uint32_t)(ny * nz);
+   if (rows > MASK_SMEM_ROWS) {
+      if (threadIdx.x == 0) recs[cell] = MaskRec{y0, y1, z0, z1, NO_MASK, {0u, 0u, 0u}};
+      return;
+   }
+   for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) C[q] = 0u;
+   __syncthreads();
+   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+      if (list_block_content(src_index, content, data, s.off + b, min_value)) {
+         const uint32_t g = gids[s.off + b];
+         const uint32_t x = g % L0;
+         const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+         atomicOr(&C[3 * (uint32_t)((z - z0) * ny + (y - y0)) + (x >> 5)], 1u << (x & 31));
+      }
+   }
+   if (threadIdx.x == 0) {
+      uint32_t off = 0u;
+      if (rows) {
+         off = atomicAdd(pool_top, 3u * rows);
+         if ((uint64_t)off + 3u * rows > pool_cap) off = NO_MASK;
+      }
+      s_off = off;
+      recs[cell] = MaskRec{y0, y1, z0, z1, off, {0u, 0u, 0u}};
+   }
+   __syncthreads();
+   const uint32_t off = s_off;
+   if (off != NO_MASK)
+      for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) pool[off + q] = C[q];
+}
+
 __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
    const uint8_t* __restrict__ content, const float* __restrict__ data, const int32_t* __restrict__ neighbors,
    uint32_t* __restrict__ out_gids, uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots,
    double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
    uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3, uint32_t n_cells,
-   uint32_t smem_rows, uint32_t* __restrict__ scratch) {
+   uint32_t smem_rows, uint32_t* __restrict__ scratch, const MaskRec* __restrict__ masks,
+   const uint32_t* __restrict__ pool) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
    __shared__ int s_box[8];
    __shared__ uint32_t s_base, s_flags;
    __shared__ double s_loss[ADJ_THREADS / 32];
+   __shared__ MaskRec s_rec[27];  // the neighbours' content masks (26: the cell's own)
 
    // persistent CTAs, one cell at a time
    for (uint32_t cell = blockIdx.x; cell < n_cells; cell += gridDim.x) {
@@ -112,25 +189,48 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       }
       s_flags = 0;
    }
+   if (threadIdx.x < 27) {
+      // mask records of the neighbours (a missing neighbour reads as empty)
+      // and of the cell itself; without masks every list is walked
+      MaskRec r{0, -1, 0, -1, NO_MASK, {0u, 0u, 0u}};
+      if (masks) {
+         const int32_t nc = (threadIdx.x < 26) ? (neighbors ? neighbors[(size_t)cell * 26 + threadIdx.x] : -1)
+                                               : (int32_t)cell;
+         r = (nc >= 0) ? masks[nc] : MaskRec{0, -1, 0, -1, 0u, {0u, 0u, 0u}};
+      }
+      s_rec[threadIdx.x] = r;
+   }
    __syncthreads();
    // pass 1: bounding boxes (y, z) of the cell's content blocks and of its
    // spatial neighbours' content blocks
    {
-      int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
-      for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-         if (list_block_content(src_index, content, data, s.off + b, min_value)) {
-            const uint32_t g = gids[s.off + b];
-            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
-            y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
+      const bool own_mask = s_rec[26].off != NO_MASK;
+      if (own_mask) {
+         if (threadIdx.x == 0) {
+            s_box[0] = s_rec[26].y0; s_box[1] = s_rec[26].y1;
+            s_box[2] = s_rec[26].z0; s_box[3] = s_rec[26].z1;
          }
+      } else {
+         int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
+         for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+            if (list_block_content(src_index, content, data, s.off + b, min_value)) {
+               const uint32_t g = gids[s.off + b];
+               const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+               y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
+            }
+         }
+         atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
+         atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
       }
-      atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
-      atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
       if (neighbors) {
          int ny0 = 1 << 20, ny1 = -1, nz0 = 1 << 20, nz1 = -1;
+         if (threadIdx.x < 26 && s_rec[threadIdx.x].off != NO_MASK && s_rec[threadIdx.x].y1 >= 0) {
+            const MaskRec& r = s_rec[threadIdx.x];
+            ny0 = r.y0; ny1 = r.y1; nz0 = r.z0; nz1 = r.z1;
+         }
          for (int q = 0; q < 26; ++q) {
             const int32_t nc = neighbors[(size_t)cell * 26 + q];
-            if (nc < 0) continue;
+            if (nc < 0 || s_rec[q].off != NO_MASK) continue;
             const CellSlot ns = slots[nc];
             for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
                if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
@@ -167,14 +267,27 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    uint32_t* prefix = base + 6 * rows;  // rows
    for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) C[q] = 0;
    __syncthreads();
-   // pass 2: content mask rows
-   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-      if (list_block_content(src_index, content, data, s.off + b, min_value)) {
-         const uint32_t g = gids[s.off + b];
-         const uint32_t x = g % L0;
-         const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
-         const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
-         atomicOr(&C[3 * r + (x >> 5)], 1u << (x & 31));
+   // pass 2: content mask rows (copied from the cell's own mask when it has one)
+   if (s_rec[26].off != NO_MASK) {
+      const MaskRec& m = s_rec[26];
+      if (m.y1 >= 0) {
+         const int my = m.y1 - m.y0 + 1;
+         const uint32_t mrows = (uint32_t)(my * (m.z1 - m.z0 + 1));
+         for (uint32_t q = threadIdx.x; q < 3 * mrows; q += blockDim.x) {
+            const uint32_t mr = q / 3, w = q - 3 * mr;
+            const int y = m.y0 + (int)(mr % my), z = m.z0 + (int)(mr / my);
+            C[3 * (uint32_t)((z - z0) * ny + (y - y0)) + w] = pool[m.off + q];
+         }
+      }
+   } else {
+      for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
+         if (list_block_content(src_index, content, data, s.off + b, min_value)) {
+            const uint32_t g = gids[s.off + b];
+            const uint32_t x = g % L0;
+            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+            const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+            atomicOr(&C[3 * r + (x >> 5)], 1u << (x & 31));
+         }
       }
    }
    __syncthreads();
@@ -210,9 +323,28 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    // blocks with content in a spatial neighbour (adjust_velocity_blocks,
    // spatial_cell_cpu.cpp:211-221)
    if (neighbors && nb_any) {
+      // neighbours with a mask: each thread ORs their rows into its own rows
+      if (masks) {
+         for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+            const int yy = y0 + (int)(r % ny), zz = z0 + (int)(r / ny);
+            uint32_t h0 = H[3 * r], h1 = H[3 * r + 1], h2 = H[3 * r + 2];
+            for (int q = 0; q < 26; ++q) {
+               const MaskRec& m = s_rec[q];
+               if (m.off == NO_MASK || yy < m.y0 || yy > m.y1 || zz < m.z0 || zz > m.z1) continue;
+               const uint32_t* src = pool + m.off + 3 * (uint32_t)((zz - m.z0) * (m.y1 - m.y0 + 1) + (yy - m.y0));
+               h0 |= src[0];
+               h1 |= src[1];
+               h2 |= src[2];
+            }
+            H[3 * r] = h0;
+            H[3 * r + 1] = h1;
+            H[3 * r + 2] = h2;
+         }
+         __syncthreads();
+      }
       for (int q = 0; q < 26; ++q) {
          const int32_t nc = neighbors[(size_t)cell * 26 + q];
-         if (nc < 0) continue;
+         if (nc < 0 || s_rec[q].off != NO_MASK) continue;
          const CellSlot ns = slots[nc];
          for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
             if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
@@ -320,15 +452,24 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
-                          uint32_t n_cells, uint32_t* scratch, int grid, cudaStream_t stream) {
+                          uint32_t n_cells, uint32_t* scratch, int grid, MaskRec* masks, uint32_t* pool,
+                          uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
    const size_t smem = adjust_smem_bytes();
    cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    if (e != cudaSuccess) return e;
+   const bool use_masks = neighbors && masks && pool && pool_top;
+   if (use_masks) {
+      e = cudaMemsetAsync(pool_top, 0, sizeof(uint32_t), stream);
+      if (e != cudaSuccess) return e;
+      content_mask_kernel<<<n_cells, MASK_THREADS, 0, stream>>>(gids, src_index, slots, content, data, mesh,
+                                                                 min_value, masks, pool, pool_top, pool_cap);
+   }
    const uint32_t g = (uint32_t)grid < n_cells ? (uint32_t)grid : n_cells;
    adjust_kernel<<<g, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
                                                     out_src, out_slots, loss, status, counters, out_capacity, mesh,
-                                                    min_value, add_width, dv3, n_cells, ADJ_SMEM_ROWS, scratch);
+                                                    min_value, add_width, dv3, n_cells, ADJ_SMEM_ROWS, scratch,
+                                                    use_masks ? masks : nullptr, pool);
    return cudaGetLastError();
 }
 

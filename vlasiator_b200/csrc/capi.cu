@@ -46,6 +46,9 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
    cudaFree(b->adj_scratch);
+   cudaFree(b->mask_recs);
+   cudaFree(b->mask_pool);
+   cudaFree(b->mask_top);
    cudaFree(b->moments_r);
    for (auto& g : b->graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -163,7 +166,8 @@ int adjust_device(vlgpu_batch* b) {
                           b->data[b->cur], b->neighbors, b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss,
                           b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
-                          (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid, b->stream));
+                          (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid,
+                          b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, b->stream));
    b->launches += 1;
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
@@ -663,6 +667,12 @@ int vlgpu_batch_set_grid(vlgpu_batch* b, const uint32_t dims[3], const double dx
       VL_CHECK(cudaMalloc(&b->item_pencil, sizeof(uint32_t) * cap));
       VL_CHECK(cudaMalloc(&b->trans_rows, sizeof(uint32_t) * b->row_cap));
       VL_CHECK(cudaMalloc(&b->trans_src, sizeof(uint32_t) * b->row_cap));
+      // content masks of the adjustment: room for 512 rows per cell on average
+      const uint64_t words = std::min<uint64_t>(3ull * 512 * b->n_cells, 0xfffffff0ull);
+      b->mask_cap = (uint32_t)words;
+      VL_CHECK(cudaMalloc(&b->mask_recs, sizeof(MaskRec) * b->n_cells));
+      VL_CHECK(cudaMalloc(&b->mask_pool, sizeof(uint32_t) * words));
+      VL_CHECK(cudaMalloc(&b->mask_top, sizeof(uint32_t)));
       VL_CHECK(cudaMalloc(&b->tcounters, sizeof(TransCounters)));
       VL_CHECK(cudaMemset(b->tcounters, 0, sizeof(TransCounters)));
    }

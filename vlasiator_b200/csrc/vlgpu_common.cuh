@@ -46,6 +46,16 @@ struct MeshDev {
    float vmin[3];
 };
 
+// Content mask of one cell for the block adjustment on a grid: the (y, z)
+// bounding box of its content blocks (y1 < 0: none) and the offset of its
+// x-mask rows (3 words per row) in the mask pool, or 0xffffffff when the rows
+// were not stored (the cell's block list is read instead).
+struct MaskRec {
+   int32_t y0, y1, z0, z1;
+   uint32_t off;
+   uint32_t pad[3];
+};
+
 // Counters of one sweep, zeroed before the columnize launch.
 struct SweepCounters {
    uint32_t n_sets;
