@@ -110,7 +110,6 @@ __global__ void __launch_bounds__(MASK_THREADS) content_mask_kernel(
    __shared__ uint32_t s_off;
    const uint32_t cell = blockIdx.x;
    const CellSlot s = slots[cell];
-   const uint32_t L0 = mesh.len[0], L1 = mesh.len[1];
    if (threadIdx.x == 0) {
       s_box[0] = 1 << 20;
       s_box[1] = -1;
@@ -123,7 +122,9 @@ __global__ void __launch_bounds__(MASK_THREADS) content_mask_kernel(
       for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
          if (list_block_content(src_index, content, data, s.off + b, min_value)) {
             const uint32_t g = gids[s.off + b];
-            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+            uint32_t bx, by, bz;
+            block_xyz(mesh, g, bx, by, bz);
+            const int y = (int)by, z = (int)bz;
             y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
          }
       }
@@ -143,8 +144,9 @@ __global__ void __launch_bounds__(MASK_THREADS) content_mask_kernel(
    for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
       if (list_block_content(src_index, content, data, s.off + b, min_value)) {
          const uint32_t g = gids[s.off + b];
-         const uint32_t x = g % L0;
-         const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+         uint32_t x, by, bz;
+         block_xyz(mesh, g, x, by, bz);
+         const int y = (int)by, z = (int)bz;
          atomicOr(&C[3 * (uint32_t)((z - z0) * ny + (y - y0)) + (x >> 5)], 1u << (x & 31));
       }
    }
@@ -215,7 +217,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
          for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
             if (list_block_content(src_index, content, data, s.off + b, min_value)) {
                const uint32_t g = gids[s.off + b];
-               const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+               uint32_t bx, by, bz;
+            block_xyz(mesh, g, bx, by, bz);
+            const int y = (int)by, z = (int)bz;
                y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
             }
          }
@@ -235,7 +239,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
             for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
                if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
                   const uint32_t g = gids[ns.off + b];
-                  const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+                  uint32_t bx, by, bz;
+            block_xyz(mesh, g, bx, by, bz);
+            const int y = (int)by, z = (int)bz;
                   ny0 = min(ny0, y); ny1 = max(ny1, y); nz0 = min(nz0, z); nz1 = max(nz1, z);
                }
             }
@@ -283,8 +289,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
          if (list_block_content(src_index, content, data, s.off + b, min_value)) {
             const uint32_t g = gids[s.off + b];
-            const uint32_t x = g % L0;
-            const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+            uint32_t x, by, bz;
+            block_xyz(mesh, g, x, by, bz);
+            const int y = (int)by, z = (int)bz;
             const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
             atomicOr(&C[3 * r + (x >> 5)], 1u << (x & 31));
          }
@@ -349,8 +356,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
          for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
             if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
                const uint32_t g = gids[ns.off + b];
-               const uint32_t x = g % L0;
-               const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+               uint32_t x, by, bz;
+               block_xyz(mesh, g, x, by, bz);
+               const int y = (int)by, z = (int)bz;
                const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
                atomicOr(&H[3 * r + (x >> 5)], 1u << (x & 31));
             }
@@ -398,8 +406,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
       const uint32_t g = gids[s.off + b];
       const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-      const uint32_t x = g % L0;
-      const int y = (int)((g / L0) % L1), z = (int)(g / (L0 * L1));
+      uint32_t x, by, bz;
+      block_xyz(mesh, g, x, by, bz);
+      const int y = (int)by, z = (int)bz;
       bool inH = false;
       uint32_t pos = 0;
       if (any && y >= y0 && y <= y1 && z >= z0 && z <= z1) {

@@ -332,6 +332,7 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
       b->mdev.dv[d] = (float)b->dv_d[d];
       b->mdev.vmin[d] = (float)mesh->vmin[d];
    }
+   set_block_reciprocals(b->mdev);
    auto fail = [&](cudaError_t e, const char* what) {
       int s = cuda_status(e, what);
       free_batch(b);

@@ -116,14 +116,13 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
                                              const float* __restrict__ data, const CellSlot s, double* out,
                                              const MeshDev& mesh, double vmin0, double vmin1, double vmin2, double bs0,
                                              double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-                                             double charge, double U0, double U1, double U2, uint32_t m0,
-                                             uint32_t m1, double* sh_hi, double* sh_lo) {
+                                             double charge, double U0, double U1, double U2, double* sh_hi,
+                                             double* sh_lo) {
    constexpr int NS = SECOND ? 10 : 4;
    const int sub = threadIdx.x & 15, grp = threadIdx.x >> 4;
    const int j = sub & 3, k = sub >> 2;
    const double cy = (j + 0.5) * dv1 - U1, cz = (k + 0.5) * dv2 - U2;
    const double cx0 = 0.5 * dv0 - U0, cx1 = 1.5 * dv0 - U0, cx2 = 2.5 * dv0 - U0, cx3 = 3.5 * dv0 - U0;
-   const uint32_t L0 = mesh.len[0], L1 = mesh.len[1];
    Kahan acc[NS];
    constexpr int MOM_UNROLL = SECOND ? 4 : 8;  // blocks in flight per thread group
    for (uint32_t b0 = grp; b0 < s.count; b0 += MOM_GROUPS * MOM_UNROLL) {
@@ -148,16 +147,7 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
 #pragma unroll
       for (int u = 0; u < MOM_UNROLL; ++u) {
          uint32_t bi, bj, bk;
-         if (m0) {  // floor divisions as multiply-high by the reciprocals m0, m1
-            const uint32_t q0 = __umulhi(g[u], m0);
-            bi = g[u] - q0 * L0;
-            bk = __umulhi(q0, m1);
-            bj = q0 - bk * L1;
-         } else {
-            bi = g[u] % L0;
-            bj = (g[u] / L0) % L1;
-            bk = g[u] / (L0 * L1);
-         }
+         block_xyz(mesh, g[u], bi, bj, bk);
          const double bx = vmin0 + bi * bs0;
          const double uy = (vmin1 + bj * bs1) + cy;
          const double uz = (vmin2 + bk * bs2) + cz;
@@ -230,7 +220,7 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
    const CellSlot* __restrict__ slots, double* moments, const double* shift, MeshDev mesh, double vmin0,
    double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-   double charge, uint32_t m0, uint32_t m1) {
+   double charge) {
    __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
    __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
    const uint32_t cell = blockIdx.x;
@@ -238,7 +228,7 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_kernel(
    const double* sh = shift + (size_t)cell * MOM_COUNT;
    const double U0 = SECOND ? sh[MOM_VX] : 0.0, U1 = SECOND ? sh[MOM_VY] : 0.0, U2 = SECOND ? sh[MOM_VZ] : 0.0;
    moments_pass<SECOND>(gids, src_index, data, slots[cell], out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1,
-                        dv2, mass, charge, U0, U1, U2, m0, m1, sh_hi, sh_lo);
+                        dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo);
 }
 
 // Both passes of a cell in one CTA: the first moments (U = 0) into `first`
@@ -251,7 +241,7 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_pair_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
    const CellSlot* __restrict__ slots, double* __restrict__ first, double* __restrict__ moments, MeshDev mesh,
    double vmin0, double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2,
-   double mass, double charge, uint32_t m0, uint32_t m1) {
+   double mass, double charge) {
    __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
    __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
    __shared__ double s_U[3];
@@ -260,7 +250,7 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_pair_kernel(
    double* out = moments + (size_t)cell * MOM_COUNT;
    double* out1 = first ? first + (size_t)cell * MOM_COUNT : out;
    moments_pass<false>(gids, src_index, data, s, out1, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
-                       charge, 0.0, 0.0, 0.0, m0, m1, sh_hi, sh_lo);
+                       charge, 0.0, 0.0, 0.0, sh_hi, sh_lo);
    if (threadIdx.x == 0) {
       s_U[0] = out1[MOM_VX];
       s_U[1] = out1[MOM_VY];
@@ -268,7 +258,7 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_pair_kernel(
    }
    __syncthreads();
    moments_pass<true>(gids, src_index, data, s, out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
-                      charge, s_U[0], s_U[1], s_U[2], m0, m1, sh_hi, sh_lo);
+                      charge, s_U[0], s_U[1], s_U[2], sh_hi, sh_lo);
 }
 
 // Per-cell acceleration inputs on the device.
@@ -380,36 +370,20 @@ cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const Cel
 }
 
 // ---------------------------------------------------------------------------
-// Reciprocals for the block-index decomposition i = g mod L0, j = (g / L0)
-// mod L1, k = g / (L0 L1): floor(n / d) = umulhi(n, floor(2^32 / d) + 1) holds
-// exactly for n < 2^32 / d (division by invariant integers, Granlund and
-// Montgomery 1994), so both are used only when every block ID and every
-// g / L0 is that small; else m0 = m1 = 0 and the kernels divide.
-static void block_index_magic(const MeshDev& mesh, uint32_t& m0, uint32_t& m1) {
-   const uint64_t L0 = mesh.len[0], L1 = mesh.len[1], L2 = mesh.len[2];
-   const uint64_t two32 = 1ull << 32;
-   m0 = m1 = 0;
-   if (L0 < 2 || L1 < 2 || L0 * L1 * L2 * L0 >= two32 || L1 * L2 * L1 >= two32) return;
-   m0 = (uint32_t)(two32 / L0 + 1);
-   m1 = (uint32_t)(two32 / L1 + 1);
-}
-
 cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
                            double* moments, const double* shift, const MeshDev& mesh, const double vmin[3],
                            const double bs[3], const double dv[3], double mass, double charge, bool second,
                            uint32_t n_cells, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
    if (!shift) shift = moments;
-   uint32_t m0, m1;
-   block_index_magic(mesh, m0, m1);
    if (second)
       moments_kernel<true><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, shift, mesh,
                                                                vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                               dv[1], dv[2], mass, charge, m0, m1);
+                                                               dv[1], dv[2], mass, charge);
    else
       moments_kernel<false><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, shift, mesh,
                                                                 vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                                dv[1], dv[2], mass, charge, m0, m1);
+                                                                dv[1], dv[2], mass, charge);
    return cudaGetLastError();
 }
 
@@ -418,11 +392,9 @@ cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
                                 double charge, uint32_t n_cells, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
-   uint32_t m0, m1;
-   block_index_magic(mesh, m0, m1);
    moments_pair_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, first, moments, mesh,
                                                            vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                           dv[1], dv[2], mass, charge, m0, m1);
+                                                           dv[1], dv[2], mass, charge);
    return cudaGetLastError();
 }
 

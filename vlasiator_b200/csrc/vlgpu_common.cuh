@@ -39,12 +39,43 @@ struct SweepCell {
    uint32_t pad;
 };
 
-// Mesh constants used on the device (cell size and origin already in Realf).
+// Mesh constants used on the device (cell size and origin already in Realf),
+// with the reciprocals of block_xyz (zero: plain division).
 struct MeshDev {
    uint32_t len[3];
    float dv[3];
    float vmin[3];
+   uint32_t m0 = 0, m1 = 0;
 };
+
+// Reciprocals for the block-index decomposition of block_xyz: floor(n / d) =
+// umulhi(n, floor(2^32 / d) + 1) holds exactly for n < 2^32 / d (division by
+// invariant integers, Granlund and Montgomery 1994), so they are set only when
+// every block ID n < L0 L1 L2 satisfies it for d = L0 and every n / L0 for
+// d = L1.
+inline void set_block_reciprocals(MeshDev& m) {
+   const uint64_t L0 = m.len[0], L1 = m.len[1], L2 = m.len[2];
+   const uint64_t two32 = 1ull << 32;
+   m.m0 = m.m1 = 0;
+   if (L0 < 2 || L1 < 2 || L0 * L1 * L2 * L0 >= two32 || L1 * L2 * L1 >= two32) return;
+   m.m0 = (uint32_t)(two32 / L0 + 1);
+   m.m1 = (uint32_t)(two32 / L1 + 1);
+}
+
+// x = g mod L0, y = (g / L0) mod L1, z = g / (L0 L1) of block ID g.
+__device__ __forceinline__ void block_xyz(const MeshDev& m, uint32_t g, uint32_t& x, uint32_t& y, uint32_t& z) {
+   if (m.m0) {
+      const uint32_t q0 = __umulhi(g, m.m0);
+      x = g - q0 * m.len[0];
+      z = __umulhi(q0, m.m1);
+      y = q0 - z * m.len[1];
+   } else {
+      const uint32_t q0 = g / m.len[0];
+      x = g - q0 * m.len[0];
+      z = q0 / m.len[1];
+      y = q0 - z * m.len[1];
+   }
+}
 
 // Content mask of one cell for the block adjustment on a grid: the (y, z)
 // bounding box of its content blocks (y1 < 0: none) and the offset of its
