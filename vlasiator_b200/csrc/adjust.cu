@@ -179,6 +179,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    __shared__ uint32_t s_base, s_flags;
    __shared__ double s_loss[ADJ_THREADS / 32];
    __shared__ MaskRec s_rec[27];  // the neighbours' content masks (26: the cell's own)
+   __shared__ uint32_t s_first[27];  // first mask-row item of each neighbour
 
    // persistent CTAs, one cell at a time
    for (uint32_t cell = blockIdx.x; cell < n_cells; cell += gridDim.x) {
@@ -330,22 +331,34 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    // blocks with content in a spatial neighbour (adjust_velocity_blocks,
    // spatial_cell_cpu.cpp:211-221)
    if (neighbors && nb_any) {
-      // neighbours with a mask: each thread ORs their rows into its own rows
+      // neighbours with a mask: one item per mask row of each neighbour (all
+      // inside the box), consecutive threads on consecutive rows of the pool
       if (masks) {
-         for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
-            const int yy = y0 + (int)(r % ny), zz = z0 + (int)(r / ny);
-            uint32_t h0 = H[3 * r], h1 = H[3 * r + 1], h2 = H[3 * r + 2];
+         if (threadIdx.x == 0) {
+            uint32_t t = 0;
             for (int q = 0; q < 26; ++q) {
+               s_first[q] = t;
                const MaskRec& m = s_rec[q];
-               if (m.off == NO_MASK || yy < m.y0 || yy > m.y1 || zz < m.z0 || zz > m.z1) continue;
-               const uint32_t* src = pool + m.off + 3 * (uint32_t)((zz - m.z0) * (m.y1 - m.y0 + 1) + (yy - m.y0));
-               h0 |= src[0];
-               h1 |= src[1];
-               h2 |= src[2];
+               if (m.off != NO_MASK && m.y1 >= 0) t += (uint32_t)((m.y1 - m.y0 + 1) * (m.z1 - m.z0 + 1));
             }
-            H[3 * r] = h0;
-            H[3 * r + 1] = h1;
-            H[3 * r + 2] = h2;
+            s_first[26] = t;
+         }
+         __syncthreads();
+         const uint32_t items = s_first[26];
+         int q = 0;
+         for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
+            while (it >= s_first[q + 1]) ++q;
+            const MaskRec& m = s_rec[q];
+            const uint32_t mr = it - s_first[q];
+            const uint32_t my = (uint32_t)(m.y1 - m.y0 + 1);
+            const uint32_t mz = mr / my;
+            const int y = m.y0 + (int)(mr - mz * my), z = m.z0 + (int)mz;
+            const uint32_t* src = pool + m.off + 3 * mr;
+            const uint32_t w0 = __ldg(src), w1 = __ldg(src + 1), w2 = __ldg(src + 2);
+            uint32_t* dst = &H[3 * (uint32_t)((z - z0) * ny + (y - y0))];
+            if (w0) atomicOr(dst, w0);
+            if (w1) atomicOr(dst + 1, w1);
+            if (w2) atomicOr(dst + 2, w2);
          }
          __syncthreads();
       }
