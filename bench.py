@@ -462,7 +462,8 @@ def run_vlasov(args):
                    "l2": "inputs larger than L2 (126 MB)",
                    "parallelism": f"{world} independent grids (no data-path collective)"},
         "gpu_launches": launches,
-        "arithmetic": "exact" if args.exact else "fused acceleration remap; translation in the reference's order",
+        "arithmetic": "exact (the reference's operation order)" if args.exact else
+        "fused acceleration remap and fused translation (1e-5 of peak per sweep)",
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                        "what": "device time of one full Vlasov step of the grid"},
         "status_cells_flagged": int((status != 0).sum()),

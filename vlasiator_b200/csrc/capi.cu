@@ -168,7 +168,7 @@ int adjust_device(vlgpu_batch* b) {
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
                           (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid,
                           b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, b->stream));
-   b->launches += 1;
+   b->launches += (b->neighbors && b->mask_recs) ? 2 : 1;  // content masks first on a grid
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
    b->st_gids = b->adj_gids[a];
