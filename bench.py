@@ -321,35 +321,59 @@ def run_ours(args):
                  "batched_over_plain": value / p_value,
                  "path": "vlgpu_accelerate_per_cell: one columnize + remap launch sequence per cell and sweep"}
 
+    batch.close()
+
     # end to end through the C ABI: host -> device copy of the step's input,
-    # the step, device -> host copy of the result (pinned host buffers)
+    # the step, device -> host copy of the result (pinned host buffers).  The
+    # cells are split into chunks, one batch (and CUDA stream) each, issued
+    # with the asynchronous upload / two-phase download so that one chunk's
+    # copies overlap the others' steps and copies in the other direction.
     h_gids = torch.from_numpy(gids).pin_memory()
     h_data = torch.from_numpy(data).pin_memory()
-    h_offs = offs.copy()
-    out_g = np.zeros(int(cap), np.uint32)
-    out_d = torch.empty((int(cap), WID3), dtype=torch.float32).pin_memory()
+    n_chunks = max(1, min(args.e2e_chunks, args.cells))
+    bounds = np.linspace(0, args.cells, n_chunks + 1).astype(np.int64)
+    chunks = []
+    for k in range(n_chunks):
+        c0, c1 = int(bounds[k]), int(bounds[k + 1])
+        b0, b1 = int(offs[c0]), int(offs[c1])
+        cap_k = int((b1 - b0) * 1.6) + 65536
+        bk = vlgpu.Batch(mesh, c1 - c0, cap_k, device=local, exact=args.exact)
+        chunks.append({"batch": bk, "offs": (offs[c0:c1 + 1] - offs[c0]).astype(np.uint64),
+                       "gids": h_gids[b0:b1].numpy(), "data": h_data[b0:b1].numpy(),
+                       "B": B[c0:c1], "dt": dt[c0:c1] if np.ndim(dt) else dt,
+                       "out_g": torch.empty(cap_k, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                       "out_d": torch.empty((cap_k, WID3), dtype=torch.float32).pin_memory().numpy()})
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     t_e2e = 0.0
     h2d = d2h = 0
     e2e_updates = 0
     for s in range(e2e_steps + 1):
         t0 = time.perf_counter()
-        batch.upload_packed(h_offs, h_gids.numpy(), h_data.numpy())
-        batch.accelerate(B, dt, orders[s % len(orders)])
-        c_off, c_cnt, g_out, d_out = batch.download_raw(out_g, out_d.numpy())
+        # every chunk's upload, step and slot read-back is queued first (the
+        # host-to-device engine never waits on the host); each download then
+        # follows as soon as its chunk's step is done
+        for ch in chunks:
+            ch["batch"].upload_async(ch["offs"], ch["gids"], ch["data"])
+            ch["batch"].accelerate(ch["B"], ch["dt"], orders[s % len(orders)])
+            ch["batch"].download_begin()
+        outs = [ch["batch"].download_end(ch["out_g"], ch["out_d"]) for ch in chunks]
+        for ch in chunks:
+            ch["batch"].sync()
         el = time.perf_counter() - t0
         if s > 0:  # the first pass warms the host paths
             t_e2e += el
             e2e_updates += WID3 * total
-            h2d += h_offs.nbytes + total * 4 + total * WID3 * 4
-            d2h += c_off.nbytes + c_cnt.nbytes + len(g_out) * (4 + WID3 * 4)
+            for ch, (c_off, c_cnt, g_out, _) in zip(chunks, outs):
+                h2d += ch["offs"].nbytes + ch["gids"].nbytes + ch["data"].nbytes
+                d2h += c_off.nbytes + c_cnt.nbytes + len(g_out) * (4 + WID3 * 4)
+    for ch in chunks:
+        ch["batch"].close()
     t_e2e = allreduce_max(pg, t_e2e)
     e2e_value = allreduce_sum(pg, float(e2e_updates)) / t_e2e
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(mesh, offs, gids, data, B, dt, orders, args.cpu_sample)
-    batch.close()
     if rank != 0:
         return 0
     line = {
@@ -375,7 +399,9 @@ def run_ours(args):
                      "algorithmic_bytes": "8 B per source phase-space cell per sweep"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(e2e_steps, 1),
                 "d2h_bytes_per_step": d2h // max(e2e_steps, 1), "steps": e2e_steps,
-                "path": "vlgpu_batch_upload + vlgpu_accelerate + vlgpu_batch_download_raw, pinned host buffers"},
+                "chunks": n_chunks,
+                "path": "per chunk of cells: vlgpu_batch_upload_async + vlgpu_accelerate + "
+                        "vlgpu_batch_download_begin / _end, pinned host buffers, chunks overlapped"},
         "clocks": clk.summary(),
     }
     if cpu is not None:
@@ -555,6 +581,7 @@ def main():
     ap.add_argument("--cells", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-chunks", type=int, default=32, help="accel e2e: batches the cells are split into")
     ap.add_argument("--cpu-sample", type=int, default=256)
     ap.add_argument("--ref-sample", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true")

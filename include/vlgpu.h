@@ -94,6 +94,20 @@ int vlgpu_batch_download(vlgpu_batch* b, uint64_t* offsets, uint32_t* gids, floa
 int vlgpu_batch_download_raw(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
                              uint64_t capacity, uint64_t* used);
 
+/* Asynchronous forms of upload and download_raw for pipelines of several
+   batches (no reference counterpart).  vlgpu_batch_upload_async does the
+   same checks as vlgpu_batch_upload but only enqueues the copies: gids and
+   data (pinned host memory for overlap) must stay untouched until the
+   batch's work is done (vlgpu_batch_sync).  vlgpu_batch_download_begin
+   enqueues the compaction of an adjusted state and the copy of the cell
+   slots; vlgpu_batch_download_end waits for those slots only, fills cell_off,
+   cell_count and *used as vlgpu_batch_download_raw does and enqueues the
+   copy of gids and data, which hold the result after vlgpu_batch_sync. */
+int vlgpu_batch_upload_async(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* gids, const float* data);
+int vlgpu_batch_download_begin(vlgpu_batch* b);
+int vlgpu_batch_download_end(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
+                             uint64_t capacity, uint64_t* used);
+
 /* Per-cell VLGPU_CELL_* bits accumulated since the last upload. */
 int vlgpu_batch_status(vlgpu_batch* b, uint32_t* status);
 

@@ -519,4 +519,36 @@ cudaError_t launch_materialize(const uint32_t* src_index, const float* src, floa
    return cudaGetLastError();
 }
 
+// The same for a row count known only on the device (*n_rows), grid-stride.
+__global__ void materialize_rows_kernel(const uint32_t* __restrict__ src_index, const float4* __restrict__ src,
+                                        float4* __restrict__ dst, const uint32_t* __restrict__ n_rows) {
+   const uint64_t n = (uint64_t)(*n_rows) * 16;
+   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+      const uint64_t p = t >> 4;
+      const uint32_t idx = src_index[p];
+      dst[t] = (idx == NO_BLOCK) ? make_float4(0.f, 0.f, 0.f, 0.f) : src[(uint64_t)idx * 16 + (t & 15)];
+   }
+}
+
+// Copies the cell slots into mapped pinned host memory: the writes travel as
+// a kernel's stores, not through the copy engine, so they do not queue behind
+// large device-to-host copies of other streams.
+__global__ void slots_to_host_kernel(const CellSlot* __restrict__ src, CellSlot* host_dst, uint32_t n) {
+   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+   if (c < n) host_dst[c] = src[c];
+}
+
+cudaError_t launch_slots_to_host(const CellSlot* src, CellSlot* host_dst, uint32_t n, cudaStream_t stream) {
+   if (n == 0) return cudaSuccess;
+   slots_to_host_kernel<<<(n + 255) / 256, 256, 0, stream>>>(src, host_dst, n);
+   return cudaGetLastError();
+}
+
+cudaError_t launch_materialize_rows(const uint32_t* src_index, const float* src, float* dst, const uint32_t* n_rows,
+                                    int grid, cudaStream_t stream) {
+   materialize_rows_kernel<<<grid, 256, 0, stream>>>(src_index, reinterpret_cast<const float4*>(src),
+                                                     reinterpret_cast<float4*>(dst), n_rows);
+   return cudaGetLastError();
+}
+
 }  // namespace vlgpu

@@ -74,6 +74,9 @@ cudaError_t launch_fill(const FillCell* cells, uint32_t n_cells, const MeshDev& 
                         CellSlot* slots, cudaStream_t stream);
 cudaError_t launch_materialize(const uint32_t* src_index, const float* src, float* dst, uint64_t n_blocks,
                                cudaStream_t stream);
+cudaError_t launch_slots_to_host(const CellSlot* src, CellSlot* host_dst, uint32_t n, cudaStream_t stream);
+cudaError_t launch_materialize_rows(const uint32_t* src_index, const float* src, float* dst, const uint32_t* n_rows,
+                                    int grid, cudaStream_t stream);
 struct TransCounters {
    uint32_t n_items;
    uint32_t work;
@@ -167,7 +170,10 @@ struct vlgpu_batch {
    // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;
    CellAccelInputs* h_accel = nullptr;
-   cudaEvent_t ev_sweep = nullptr, ev_accel = nullptr;
+   vlgpu::CellSlot* h_slots_in = nullptr;   // n_cells slots and the row count of an asynchronous upload
+   vlgpu::CellSlot* h_slots_out = nullptr;  // n_cells slots of an asynchronous download (mapped pinned)
+   vlgpu::CellSlot* d_slots_out = nullptr;  // its device address
+   cudaEvent_t ev_sweep = nullptr, ev_accel = nullptr, ev_upload = nullptr, ev_slots = nullptr;
    // captured step sequences (vlgpu_batch_capture): the executable graph and
    // the buffer state it starts and ends in
    struct GraphSlot {
@@ -208,6 +214,7 @@ int moments_device(vlgpu_batch* b, bool second, double* record = nullptr, const 
 int moments_pair_device(vlgpu_batch* b, double* first, double* record);
 int adjust_device(vlgpu_batch* b);
 int materialize(vlgpu_batch* b);
+int materialize_async(vlgpu_batch* b);
 int geometry_device(vlgpu_batch* b, uint32_t map_order);
 int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool next_pivot = true);
 int translate_device(vlgpu_batch* b, uint32_t dim, double dt);

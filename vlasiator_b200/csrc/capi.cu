@@ -55,6 +55,10 @@ void free_batch(vlgpu_batch* b) {
    for (cudaEvent_t e : b->prof_events) cudaEventDestroy(e);
    cudaFreeHost(b->h_sweep);
    cudaFreeHost(b->h_accel);
+   cudaFreeHost(b->h_slots_in);
+   cudaFreeHost(b->h_slots_out);
+   if (b->ev_upload) cudaEventDestroy(b->ev_upload);
+   if (b->ev_slots) cudaEventDestroy(b->ev_slots);
    if (b->ev_sweep) cudaEventDestroy(b->ev_sweep);
    if (b->ev_accel) cudaEventDestroy(b->ev_accel);
    if (b->stream) cudaStreamDestroy(b->stream);
@@ -197,6 +201,20 @@ int materialize(vlgpu_batch* b) {
    b->st_src = nullptr;
    b->cur = dst;
    b->pivot_valid = false;
+   return VLGPU_OK;
+}
+
+// The same without a host round trip: the row count stays on the device.
+int materialize_async(vlgpu_batch* b) {
+   if (!b->st_src) return VLGPU_OK;
+   const int dst = 1 - b->cur;
+   VL_CHECK(launch_materialize_rows(b->st_src, b->data[b->cur], b->data[dst], b->rows_used + b->st_list,
+                                    b->sm_count * 8, b->stream));
+   b->launches += 1;
+   VL_CHECK(cudaMemcpyAsync(b->rows_used + dst, b->rows_used + b->st_list, sizeof(uint32_t),
+                            cudaMemcpyDeviceToDevice, b->stream));
+   b->st_src = nullptr;
+   b->cur = dst;
    return VLGPU_OK;
 }
 
@@ -384,6 +402,12 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMallocHost(&b->h_accel, sizeof(CellAccelInputs) * n_cells)) != cudaSuccess) return fail(e, "pinned");
    if ((e = cudaEventCreateWithFlags(&b->ev_sweep, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
    if ((e = cudaEventCreateWithFlags(&b->ev_accel, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+   if ((e = cudaMallocHost(&b->h_slots_in, sizeof(CellSlot) * (n_cells + 1))) != cudaSuccess) return fail(e, "pinned");
+   if ((e = cudaHostAlloc(&b->h_slots_out, sizeof(CellSlot) * n_cells, cudaHostAllocMapped)) != cudaSuccess)
+      return fail(e, "pinned");
+   if ((e = cudaHostGetDevicePointer(&b->d_slots_out, b->h_slots_out, 0)) != cudaSuccess) return fail(e, "pinned");
+   if ((e = cudaEventCreateWithFlags(&b->ev_upload, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+   if ((e = cudaEventCreateWithFlags(&b->ev_slots, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
    set_direct_state(b, 0);
    *out = b;
    return VLGPU_OK;
@@ -427,6 +451,67 @@ int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* 
    }
    set_direct_state(b, 0);
    b->content_valid = false;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_upload_async(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* gids, const float* data) {
+   if (!b || !offsets) return VLGPU_EINVAL;
+   const uint64_t total = offsets[b->n_cells];
+   if (total > b->capacity) return VLGPU_ENOMEM;
+   if (total > 0 && (!gids || !data)) return VLGPU_EINVAL;
+   for (uint32_t c = 0; c < b->n_cells; ++c)
+      if (offsets[c + 1] < offsets[c]) return VLGPU_EINVAL;
+   const uint32_t maxgid = b->mesh.len[0] * b->mesh.len[1] * b->mesh.len[2];
+   for (uint64_t q = 0; q < total; ++q)
+      if (gids[q] >= maxgid) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaEventSynchronize(b->ev_upload));  // the previous upload has read the staging buffer
+   CellSlot* hs = b->h_slots_in;
+   for (uint32_t c = 0; c < b->n_cells; ++c) hs[c] = CellSlot{(uint32_t)offsets[c], (uint32_t)(offsets[c + 1] - offsets[c])};
+   hs[b->n_cells] = CellSlot{(uint32_t)total, 0u};
+   if (total > 0) {
+      VL_CHECK(cudaMemcpyAsync(b->gids[0], gids, sizeof(uint32_t) * total, cudaMemcpyHostToDevice, b->stream));
+      VL_CHECK(cudaMemcpyAsync(b->data[0], data, sizeof(float) * WID3 * total, cudaMemcpyHostToDevice, b->stream));
+   }
+   VL_CHECK(cudaMemcpyAsync(b->slots[0], hs, sizeof(CellSlot) * b->n_cells, cudaMemcpyHostToDevice, b->stream));
+   VL_CHECK(cudaMemcpyAsync(b->rows_used, &hs[b->n_cells].off, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+   VL_CHECK(cudaMemsetAsync(b->status, 0, sizeof(uint32_t) * b->n_cells, b->stream));
+   VL_CHECK(cudaMemsetAsync(b->loss, 0, sizeof(double) * b->n_cells, b->stream));
+   VL_CHECK(cudaEventRecord(b->ev_upload, b->stream));
+   set_direct_state(b, 0);
+   b->content_valid = false;
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_download_begin(vlgpu_batch* b) {
+   if (!b) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   const int st = materialize_async(b);
+   if (st != VLGPU_OK) return st;
+   VL_CHECK(launch_slots_to_host(b->st_slots, b->d_slots_out, b->n_cells, b->stream));
+   b->launches += 1;
+   VL_CHECK(cudaEventRecord(b->ev_slots, b->stream));
+   return VLGPU_OK;
+}
+
+int vlgpu_batch_download_end(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
+                             uint64_t capacity, uint64_t* used) {
+   if (!b || !cell_off || !cell_count || !used) return VLGPU_EINVAL;
+   VL_CHECK(cudaSetDevice(b->device));
+   VL_CHECK(cudaEventSynchronize(b->ev_slots));
+   uint64_t hi = 0;
+   for (uint32_t c = 0; c < b->n_cells; ++c) {
+      cell_off[c] = b->h_slots_out[c].off;
+      cell_count[c] = b->h_slots_out[c].count;
+      hi = std::max<uint64_t>(hi, (uint64_t)cell_off[c] + cell_count[c]);
+   }
+   *used = hi;
+   if (hi > capacity) return VLGPU_ENOMEM;
+   if (hi > 0 && (!gids || !data)) return VLGPU_EINVAL;
+   if (hi > 0) {
+      VL_CHECK(cudaMemcpyAsync(gids, b->st_gids, sizeof(uint32_t) * hi, cudaMemcpyDeviceToHost, b->stream));
+      VL_CHECK(cudaMemcpyAsync(data, b->data[b->cur], sizeof(float) * WID3 * hi, cudaMemcpyDeviceToHost, b->stream));
+   }
    return VLGPU_OK;
 }
 

@@ -87,6 +87,9 @@ SIGNATURES = {
     "vlgpu_batch_stats2": (ctypes.c_int, [_vp, _u64p]),
     "vlgpu_batch_download_raw": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_sync": (ctypes.c_int, [_vp]),
+    "vlgpu_batch_upload_async": (ctypes.c_int, [_vp, _u64p, _u32p, _fp]),
+    "vlgpu_batch_download_begin": (ctypes.c_int, [_vp]),
+    "vlgpu_batch_download_end": (ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _fp, ctypes.c_uint64, _u64p]),
     "vlgpu_batch_set_exact": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_set_reconstruction": (ctypes.c_int, [_vp, ctypes.c_int]),
     "vlgpu_batch_capture": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, _u32p, ctypes.c_double]),
@@ -256,6 +259,31 @@ class Batch:
         u = int(used.value)
         return off, cnt, gids_out[:u], data_out[:u]
 
+    def upload_async(self, offsets, gids, data):
+        """Enqueues the upload; the arrays (pinned for overlap) are kept
+        referenced here until the next sync."""
+        offs = np.ascontiguousarray(offsets, np.uint64)
+        gids = np.ascontiguousarray(gids, np.uint32)
+        data = np.ascontiguousarray(data, np.float32)
+        self._inflight = (offs, gids, data)
+        _check(self.lib.vlgpu_batch_upload_async(self.h, _p(offs, ctypes.c_uint64), _p(gids, ctypes.c_uint32),
+                                                 _p(data, ctypes.c_float)), "vlgpu_batch_upload_async")
+
+    def download_begin(self):
+        _check(self.lib.vlgpu_batch_download_begin(self.h), "vlgpu_batch_download_begin")
+
+    def download_end(self, gids_out, data_out):
+        """(cell_off, cell_count, gids, data) as download_raw; gids and data
+        hold the result after sync()."""
+        off = np.zeros(self.n_cells, np.uint32)
+        cnt = np.zeros(self.n_cells, np.uint32)
+        used = ctypes.c_uint64(0)
+        _check(self.lib.vlgpu_batch_download_end(self.h, _p(off, ctypes.c_uint32), _p(cnt, ctypes.c_uint32),
+                                                 _p(gids_out, ctypes.c_uint32), _p(data_out, ctypes.c_float),
+                                                 len(gids_out), ctypes.byref(used)), "vlgpu_batch_download_end")
+        u = int(used.value)
+        return off, cnt, gids_out[:u], data_out[:u]
+
     def cells(self):
         offs, g, d = self.download()
         return [(g[offs[c]:offs[c + 1]], d[offs[c]:offs[c + 1]]) for c in range(self.n_cells)]
@@ -272,35 +300,34 @@ class Batch:
                "vlgpu_accelerate_with_intersections")
 
     def _fields(self, B, dt, curl, egradpe):
+        """vlgpu_cell_fields records (B, curl, egradpe: 9 doubles per cell) as
+        one contiguous array, and dt per cell; keep F alive for the call."""
         n = self.n_cells
-        F = (CFieldsT * n)()
-        B = np.asarray(B, np.float64).reshape(n, 3)
-        curl = np.zeros((n, 3)) if curl is None else np.asarray(curl, np.float64).reshape(n, 3)
-        eg = np.zeros((n, 3)) if egradpe is None else np.asarray(egradpe, np.float64).reshape(n, 3)
-        for c in range(n):
-            for r in range(3):
-                F[c].B[r], F[c].curl[r], F[c].egradpe[r] = B[c, r], curl[c, r], eg[c, r]
+        F = np.zeros((n, 9), np.float64)
+        F[:, 0:3] = np.asarray(B, np.float64).reshape(n, 3)
+        if curl is not None:
+            F[:, 3:6] = np.asarray(curl, np.float64).reshape(n, 3)
+        if egradpe is not None:
+            F[:, 6:9] = np.asarray(egradpe, np.float64).reshape(n, 3)
+        assert ctypes.sizeof(CFieldsT) == 9 * 8
         dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (n,)))
         return F, dt
 
+    @staticmethod
+    def _fp(F):
+        return F.ctypes.data_as(ctypes.POINTER(CFieldsT))
+
     def compute_intersections(self, B, dt, map_order: int, curl=None, egradpe=None) -> np.ndarray:
         F, dt = self._fields(B, dt, curl, egradpe)
-        _check(self.lib.vlgpu_compute_intersections(self.h, F, _p(dt, ctypes.c_double), map_order),
+        _check(self.lib.vlgpu_compute_intersections(self.h, self._fp(F), _p(dt, ctypes.c_double), map_order),
                "vlgpu_compute_intersections")
         return self.intersections()
 
     def accelerate(self, B, dt, map_order: int, curl=None, egradpe=None):
         """One acceleration step (moments -> FP64 geometry -> sweeps -> adjust -> moments) of every cell."""
-        n = self.n_cells
-        F = (CFieldsT * n)()
-        B = np.asarray(B, np.float64).reshape(n, 3)
-        curl = np.zeros((n, 3)) if curl is None else np.asarray(curl, np.float64).reshape(n, 3)
-        eg = np.zeros((n, 3)) if egradpe is None else np.asarray(egradpe, np.float64).reshape(n, 3)
-        for c in range(n):
-            for r in range(3):
-                F[c].B[r], F[c].curl[r], F[c].egradpe[r] = B[c, r], curl[c, r], eg[c, r]
-        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (n,)))
-        _check(self.lib.vlgpu_accelerate(self.h, F, _p(dt, ctypes.c_double), map_order), "vlgpu_accelerate")
+        F, dt = self._fields(B, dt, curl, egradpe)
+        _check(self.lib.vlgpu_accelerate(self.h, self._fp(F), _p(dt, ctypes.c_double), map_order),
+               "vlgpu_accelerate")
 
     def accelerate_device(self, map_order: int, per_cell: bool = False):
         fn = self.lib.vlgpu_accelerate_per_cell if per_cell else self.lib.vlgpu_accelerate_device
@@ -321,7 +348,7 @@ class Batch:
     def vlasov_step(self, B, dt: float, map_order: int, curl=None, egradpe=None):
         """Translation z, x, y + "_R" moments, then one acceleration step (grid batches)."""
         F, _ = self._fields(B, dt, curl, egradpe)
-        _check(self.lib.vlgpu_vlasov_step(self.h, F, float(dt), map_order), "vlgpu_vlasov_step")
+        _check(self.lib.vlgpu_vlasov_step(self.h, self._fp(F), float(dt), map_order), "vlgpu_vlasov_step")
 
     def vlasov_step_device(self, dt: float, map_order: int):
         _check(self.lib.vlgpu_vlasov_step_device(self.h, float(dt), map_order), "vlgpu_vlasov_step_device")
@@ -406,3 +433,4 @@ class Batch:
 
     def sync(self):
         _check(self.lib.vlgpu_batch_sync(self.h), "vlgpu_batch_sync")
+        self._inflight = None
