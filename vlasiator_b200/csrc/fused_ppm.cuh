@@ -6,13 +6,13 @@
 namespace vlgpu {
 
 // The same coefficients in plain single precision (fused mode): the superbee
-// slope as sign(a) * max(min(|a|, 2|b|), min(2|a|, |b|)) when a and b share a
-// sign (equal to maxmod(minmod(a, 2b), minmod(2a, b))), on unscaled values
-// with sign tests instead of products, and contractible arithmetic.
+// slope as sign(a) * max(min(|a|, 2|b|), min(2|a|, |b|)) when a b > 0 (equal
+// to maxmod(minmod(a, 2b), minmod(2a, b)), whose minmod tests the same
+// product), on unscaled values, with contractible arithmetic.
 __device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, float fl, float fr, float& a0,
                                                 float& a1, float& a2) {
    const float a = vp1 - v0, b = v0 - vm1;
-   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const bool same = a * b > 0.0f;
    const float aa = fabsf(a), ab = fabsf(b);
    const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
    if (sl == 0.0f) {
@@ -38,10 +38,10 @@ __device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, 
 }
 
 // Superbee slope of (l, m, r) on unscaled values: sign(a) * max(min(|a|, 2|b|),
-// min(2|a|, |b|)) when a = r - m and b = m - l share a sign, else 0.
+// min(2|a|, |b|)) when a b > 0 (a = r - m, b = m - l), else 0.
 __device__ __forceinline__ float superbee_fused(float l, float m, float r) {
    const float a = r - m, b = m - l;
-   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const bool same = a * b > 0.0f;
    const float aa = fabsf(a), ab = fabsf(b);
    return same ? copysignf(fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)), a) : 0.0f;
 }
@@ -173,7 +173,7 @@ __device__ __forceinline__ float2 h4_face_x2(float2 vm2, float2 vm1, float2 v0, 
 // Superbee slope magnitude of one cell (zero at an extremum), the faces
 // flattened to v0 where it is zero, and half the signed slope.
 __device__ __forceinline__ float half_slope(float a, float b, float v0, float& fl, float& fr) {
-   const bool same = ((__float_as_int(a) ^ __float_as_int(b)) >= 0) & (a != 0.0f) & (b != 0.0f);
+   const bool same = a * b > 0.0f;
    const float aa = fabsf(a), ab = fabsf(b);
    const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
    if (sl == 0.0f) {
