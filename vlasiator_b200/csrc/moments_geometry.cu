@@ -125,14 +125,21 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
    const double cx0 = 0.5 * dv0 - U0, cx1 = 1.5 * dv0 - U0, cx2 = 2.5 * dv0 - U0, cx3 = 3.5 * dv0 - U0;
    Kahan acc[NS];
    constexpr int MOM_UNROLL = SECOND ? 4 : 8;  // blocks in flight per thread group
-   for (uint32_t b0 = grp; b0 < s.count; b0 += MOM_GROUPS * MOM_UNROLL) {
-      uint32_t g[MOM_UNROLL], idx[MOM_UNROLL];
+   constexpr uint32_t STEP = MOM_GROUPS * MOM_UNROLL;
+   // block IDs and data indices of a batch; the next batch's are loaded while
+   // the current batch's data is in flight, so a batch waits on one round
+   // trip to memory, not on the index lookup before it
+   uint32_t g[MOM_UNROLL], idx[MOM_UNROLL];
+   auto fetch = [&](uint32_t b0, uint32_t* gg, uint32_t* ii) {
 #pragma unroll
       for (int u = 0; u < MOM_UNROLL; ++u) {
          const uint32_t b = b0 + u * MOM_GROUPS;
-         g[u] = (b < s.count) ? __ldg(gids + s.off + b) : 0u;
-         idx[u] = (b < s.count) ? (src_index ? __ldg(src_index + s.off + b) : s.off + b) : 0xffffffffu;
+         gg[u] = (b < s.count) ? __ldg(gids + s.off + b) : 0u;
+         ii[u] = (b < s.count) ? (src_index ? __ldg(src_index + s.off + b) : s.off + b) : 0xffffffffu;
       }
+   };
+   fetch(grp, g, idx);
+   for (uint32_t b0 = grp; b0 < s.count; b0 += STEP) {
       float4 f4[MOM_UNROLL];
 #pragma unroll
       for (int u = 0; u < MOM_UNROLL; ++u) {
@@ -140,6 +147,8 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
          if (idx[u] != 0xffffffffu)  // an added block holds zeros
             f4[u] = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx[u] * WID3) + sub);
       }
+      uint32_t g_next[MOM_UNROLL], idx_next[MOM_UNROLL];
+      fetch(b0 + STEP, g_next, idx_next);
       // the batch's blocks are summed plainly, the batch sums compensated
       double t[NS];
 #pragma unroll
@@ -171,6 +180,11 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
       }
 #pragma unroll
       for (int q = 0; q < NS; ++q) acc[q].add(t[q]);
+#pragma unroll
+      for (int u = 0; u < MOM_UNROLL; ++u) {
+         g[u] = g_next[u];
+         idx[u] = idx_next[u];
+      }
    }
    double hi[NS], lo[NS];
 #pragma unroll
