@@ -186,6 +186,31 @@ def cpu_reference_rate(mesh, offs, gids, data, B, dt, orders, sample_cells, targ
     return updates / elapsed, cores, f"{n} of the workload's cells x {reps} steps ({updates} cell-updates)", kind
 
 
+def cpu_vlasov_rate(dims, target_s=12.0):
+    """Times the oracle's full Vlasov step (the C restatement driven per cell,
+    one host thread) on a small grid of the same sine-wave workload; returns
+    (cell-updates/s, cores, sample description)."""
+    from oracle.oracle import Restatement  # CPU baseline leg only
+    from vlasiator_b200.projects import sinewave_grid
+    mesh = VelocityMesh()
+    cells = sinewave_grid(dims, mesh)
+    orc = Restatement("sp")
+    B = np.stack([c.B for c in cells])
+    state = [(c.gids, c.data) for c in cells]
+    dt = 0.2
+    updates, elapsed, steps = 0, 0.0, 0
+    while elapsed < target_s and steps < 50:
+        blocks = sum(len(g) for g, _ in state)
+        t0 = time.perf_counter()
+        state, _, _, _, _ = orc.vlasov_step(mesh, dims, state, B, dt, steps % 3, (3e5, 3e5, 3e5), MASS_PROTON,
+                                            CHARGE)
+        elapsed += time.perf_counter() - t0
+        updates += WID3 * blocks
+        steps += 1
+    return updates / elapsed, 1, (f"{dims[0]}x{dims[1]}x{dims[2]} grid of the same workload x {steps} steps "
+                                  f"({updates} cell-updates), oracle restatement, one thread")
+
+
 def run_reference_arm(args):
     world, rank, local, pg = dist_setup()
     if rank != 0:
@@ -503,6 +528,9 @@ def run_vlasov(args):
     t_e2e = allreduce_max(pg, t_e2e)
     e2e_value = allreduce_sum(pg, float(e_upd)) / t_e2e
     batch.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_vlasov_rate((8, 4, 2))
     if rank != 0:
         return 0
     line = {
@@ -529,6 +557,9 @@ def run_vlasov(args):
                                           "moments)"},
         "clocks": clk.summary(),
     }
+    if cpu is not None:
+        rate, cores, sample = cpu
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     print(json.dumps(line))
     return 0
 
