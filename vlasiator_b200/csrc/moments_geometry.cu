@@ -98,10 +98,10 @@ __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* s
 // One CTA per cell; 16 threads per velocity block, each owning one x-row of
 // four cells (a float4: i = 0..3 at j = sub & 3, k = sub >> 2), and every
 // thread group keeps MOM_UNROLL blocks in flight.  With SECOND, velocities
-// are taken relative to a reference velocity U (the cell's bulk velocity in
-// its moment record, written by the first-moments pass that precedes every
-// second-moments pass), so one pass over the data gives both the first
-// moments and the central second moments:
+// are taken relative to a reference velocity U (a bulk velocity of the same
+// or of the previous VDF of the cell: the first pass of the moments pair, or
+// the acceleration step's pivot), so one pass over the data gives both the
+// first moments and the central second moments:
 //   S0 = sum f, S_a = sum f u_a, S_ab = sum f u_a u_b   (u = v - U)
 //   n V_a = (S_a + U_a S0) dv^3,  P_ab = m dv^3 (S_ab - S_a S_b / S0).
 // With U close to V the correction term is small, so nothing cancels; the

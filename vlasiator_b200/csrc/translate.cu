@@ -415,18 +415,9 @@ __device__ __forceinline__ void plane_shift(uint32_t sw2, int k, float dvz, floa
    z2 = up ? 1.0f : -zt;
 }
 
-// The outgoing integral of one column of window cell j (2 <= j <= W-3) given
-// its left and right faces; zero when the plane is skipped.
-__device__ __forceinline__ float outgoing(float vm1, float v0, float vp1, float fl, float fr, float z1, float z2,
-                                          bool active) {
-   float a0, a1, a2;
-   ppm_coeff_fused(vm1, v0, vp1, fl, fr, a0, a1, a2);
-   const float ngbr = z2 * fmaf(z2, fmaf(z2, a2, a1), a0) - z1 * fmaf(z1, fmaf(z1, a2, a1), a0);
-   return active ? ngbr : 0.0f;
-}
-
-// ppm_coeff_fused and the outgoing integral over [z1, z2] for two columns;
-// zero for a column whose plane is skipped.
+// The PPM (ppm_coeff_x2) and the outgoing integral over [z1, z2] of two
+// columns given their left and right faces; zero for a column whose plane is
+// skipped.
 __device__ __forceinline__ float2 outgoing_x2(float2 vm1, float2 v0, float2 vp1, float2 fl, float2 fr, float2 z1,
                                               float2 z2, uint32_t act_x, uint32_t act_y) {
    float2 a0, a1, a2;
