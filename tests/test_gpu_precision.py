@@ -100,7 +100,7 @@ def test_fp32_gpu_against_fp64_oracle(vl_lib, mesh, fp64_run, exact):
     m64 = sum(float(d.sum()) for _, d in fp64_run["state"]) * dv3(mesh) + fp64_run["loss"]
     drift32, drift64 = m32 / m0 - 1, m64 / m0 - 1
     mode = "exact" if exact else "fused"
-    print(f"\nprecision study ({mode} remap, grid {DIMS}, {STEPS} steps, dt {dt:.4f} s):"
+    print(f"\nprecision study ({mode} mode: remap and translation, grid {DIMS}, {STEPS} steps, dt {dt:.4f} s):"
           f"\n  VDF max |err| / peak at the end: {vdf_err:.3e}"
           f"\n  n rel err: step 1 {n_err[0]:.2e}, step {STEPS} {n_err[-1]:.2e}, max {n_err.max():.2e}"
           f"\n  V err / max|V|: step 1 {v_err[0]:.2e}, step {STEPS} {v_err[-1]:.2e}"
