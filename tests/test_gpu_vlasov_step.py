@@ -155,3 +155,31 @@ def test_vlasov_step_matches_oracle(vl, mesh, orc_sp, exact):
     m0 = sum(float(c.data.astype(np.float64).sum()) for c in cells)
     m1 = sum(float(d.astype(np.float64).sum()) for _, d in got["cells"])
     assert abs(m1 / m0 - 1.0) < 1e-3
+
+
+def test_spatial_adjust_with_a_wide_cell(vl, mesh, orc_sp):
+    """One hot cell whose content box (about 48 x 48 rows of y, z) exceeds
+    the adjustment's shared-memory mask and the content-mask limit: that cell
+    is adjusted with global scratch masks and its neighbours read its block
+    list instead of its mask."""
+    dims = (3, 2, 2)
+    cells = varied_grid(mesh, dims, seed=9)
+    cells[4] = maxwellian_cell(mesh, 1e6, 1e8, (1e5, 0.0, -1e5))
+    box = np.unique(cells[4].gids // mesh.length[0])  # (y, z) rows of the hot cell
+    assert len(box) > 1600
+    # every cell of this small periodic grid neighbours the hot one and
+    # takes its content blocks
+    total = sum(c.n_blocks for c in cells)
+    with vl.Batch(mesh, len(cells), len(cells) * cells[4].n_blocks + 4 * total + 65536) as b:
+        b.upload([c.gids for c in cells], [c.data for c in cells])
+        b.set_grid(dims, DX)
+        b.adjust()
+        got = b.cells()
+        loss = b.rho_loss()
+        b.sync()
+        assert not b.status().any()
+    ref, ref_loss = orc_sp.adjust_grid(mesh, dims, [(c.gids, c.data) for c in cells], 1e-15)
+    for ci in range(len(cells)):
+        np.testing.assert_array_equal(got[ci][0], ref[ci][0], err_msg=f"cell {ci}")
+        assert np.array_equal(got[ci][1], ref[ci][1]), f"cell {ci}"
+        assert loss[ci] == pytest.approx(ref_loss[ci], rel=1e-12, abs=1e-300)
