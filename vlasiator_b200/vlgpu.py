@@ -169,6 +169,7 @@ class Batch:
         _check(self.lib.vlgpu_batch_create(ctypes.byref(m), ctypes.byref(self.params), self.n_cells, self.capacity,
                                            device, ctypes.byref(h)), "vlgpu_batch_create")
         self.h = h
+        self._inflight = None  # host arrays an asynchronous upload still reads
         self.set_reconstruction(recon)
         self.set_exact(exact)
 
@@ -194,8 +195,9 @@ class Batch:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.vlgpu_batch_destroy(self.h)
+            self.lib.vlgpu_batch_destroy(self.h)  # waits for the batch's stream
             self.h = None
+        self._inflight = None
 
     def __del__(self):
         try:
