@@ -123,10 +123,13 @@ def test_translation_conserves_mass_with_common_blocks(vl, mesh):
     assert abs(m1 / m0 - 1.0) < 1e-6
 
 
-@pytest.mark.parametrize("dim,dt", [(0, 0.05), (1, -0.04), (2, 0.03)])
-def test_fused_translation_within_tolerance(vl, mesh, orc_sp, dim, dt):
-    grid = (6, 3, 2)
-    cells = grid_cells(mesh, grid, seed=40 + dim)
+@pytest.mark.parametrize("grid,dim,dt", [((6, 3, 2), 0, 0.05), ((6, 3, 2), 1, -0.04), ((6, 3, 2), 2, 0.03),
+                                         ((1, 2, 3), 0, 0.05), ((1, 2, 3), 1, -0.05), ((1, 2, 3), 2, 0.04),
+                                         ((20, 2, 1), 0, -0.03)])
+def test_fused_translation_within_tolerance(vl, mesh, orc_sp, grid, dim, dt):
+    """Pencils of 1 to 20 cells: the walk's window wraps around a short
+    pencil several times, and a 20-cell pencil takes three batches."""
+    cells = grid_cells(mesh, grid, seed=40 + dim + sum(grid))
     state = [(c.gids, c.data) for c in cells]
     total = sum(c.n_blocks for c in cells)
     with vl.Batch(mesh, len(cells), 2 * total + 4096) as b:
