@@ -7,6 +7,13 @@
 // leave a direct state (block b of a cell is data row off+b).  Block
 // adjustment leaves an indirect state (a new list whose entries point at the
 // kept rows, or at no row for added zero blocks), so it moves no VDF data.
+//
+// The acceleration transform's pivot (the first moments of the current VDF)
+// sits in its own record; pivot_valid says it describes the current state.
+// Every change of the state clears it (set_direct_state, adjustment,
+// materialisation, serving admissions), and the moments pairs that end an
+// acceleration step or compute the Vlasov step's "_R" moments set it, so the
+// next step skips its separate first-moments pass.
 #pragma once
 #include <algorithm>
 #include <cstdio>
