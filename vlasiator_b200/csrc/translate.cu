@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(TR_THREADS) trans_remap_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// fused translation remap: one warp per unit (item, L consecutive cells)
+// fused translation remap: one warp per item (pencil, block ID)
 // ---------------------------------------------------------------------------
 constexpr int TF_THREADS = 256;
 constexpr int TF_BATCH = 8;  // cells per batch of the walk (16 measured slower)
@@ -435,8 +435,8 @@ __device__ __forceinline__ float2 load_column_pair(const float* __restrict__ src
                            : make_float2(0.0f, 0.0f);
 }
 
-// Bit 0 of the result: the plane of this lane's first (second) column holds
-// a positive value in (x, y).
+// px (py) = 1 when the plane of this lane's first (second) column holds a
+// positive value in this cell's block, over the whole warp.
 template <int DIM>
 __device__ __forceinline__ void plane_positive(float2 v, uint32_t pmask, uint32_t& px, uint32_t& py) {
    if (DIM == 0) {
