@@ -11,9 +11,9 @@
 // The acceleration transform's pivot (the first moments of the current VDF)
 // sits in its own record; pivot_valid says it describes the current state.
 // Every change of the state clears it (set_direct_state, adjustment,
-// materialisation, serving admissions), and the moments pairs that end an
-// acceleration step or compute the Vlasov step's "_R" moments set it, so the
-// next step skips its separate first-moments pass.
+// materialisation, serving admissions), and the single-read moments that end
+// an acceleration step or compute the Vlasov step's "_R" moments set it, so
+// the next step skips its separate first-moments pass.
 #pragma once
 #include <algorithm>
 #include <cstdio>
@@ -46,8 +46,8 @@ cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, cons
                            double* moments, const double* shift, const MeshDev& mesh, const double vmin[3],
                            const double bs[3], const double dv[3], double mass, double charge, bool second,
                            uint32_t n_cells, cudaStream_t stream);
-cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index, const float* data,
-                                const CellSlot* slots, double* first, double* moments, const MeshDev& mesh,
+cudaError_t launch_moments_both(const uint32_t* gids, const uint32_t* src_index, const float* data,
+                                const CellSlot* slots, double* pivot, double* moments, const MeshDev& mesh,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
                                 double charge, uint32_t n_cells, cudaStream_t stream);
 cudaError_t launch_geometry(const CellAccelInputs* in, const double* moments, double* isect12, SweepCell* sweep3,
@@ -218,7 +218,7 @@ void free_batch(vlgpu_batch* b);
 void set_direct_state(vlgpu_batch* b, int pool);
 int sweep_device(vlgpu_batch* b, const vlgpu::SweepCell* sweep_cells, uint32_t dim, bool per_cell, bool first_of_step);
 int moments_device(vlgpu_batch* b, bool second, double* record = nullptr, const double* shift = nullptr);
-int moments_pair_device(vlgpu_batch* b, double* first, double* record);
+int moments_both_device(vlgpu_batch* b, double* record);
 int adjust_device(vlgpu_batch* b);
 int materialize(vlgpu_batch* b);
 int materialize_async(vlgpu_batch* b);

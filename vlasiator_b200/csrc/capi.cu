@@ -151,13 +151,15 @@ int moments_device(vlgpu_batch* b, bool second, double* record, const double* sh
    return VLGPU_OK;
 }
 
-// First moments into `first` (nullptr: into `record`), then the second
-// moments about that bulk velocity into `record`, in one launch.
-int moments_pair_device(vlgpu_batch* b, double* first, double* record) {
+// First and second moments of the current VDF in one read: the second about
+// the bulk velocity in the pivot record (any earlier VDF's, or zero), which
+// then receives this VDF's first moments; the full record goes to `record`.
+int moments_both_device(vlgpu_batch* b, double* record) {
    b->launches += 1;
-   VL_CHECK(launch_moments_pair(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, first, record, b->mdev,
+   VL_CHECK(launch_moments_both(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, b->pivot, record, b->mdev,
                                 b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, b->n_cells,
                                 b->stream));
+   b->pivot_valid = true;
    return VLGPU_OK;
 }
 
@@ -220,9 +222,9 @@ int materialize_async(vlgpu_batch* b) {
 
 // Pivot moments and the per-cell FP64 geometry of one acceleration step.
 int geometry_device(vlgpu_batch* b, uint32_t map_order) {
-   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420);
-   // a moments pair that ran on this VDF (the previous step's final moments,
-   // the Vlasov step's "_R" moments) has already written it
+   // pivot velocity from the current VDF (calculateMoments_V, vlasovmover.cpp:420),
+   // unless the moments that ended the previous step or the Vlasov step's "_R"
+   // moments already wrote it for this VDF
    if (!b->pivot_valid) {
       const int st = moments_device(b, false, b->pivot);
       if (st != VLGPU_OK) return st;
@@ -251,7 +253,7 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool ne
    // of the new VDF as the next step's pivot; else one pass about the pivot
    // velocity of this step
    if (!next_pivot) return moments_device(b, true, b->moments, b->pivot);
-   st = moments_pair_device(b, b->pivot, b->moments);
+   st = moments_both_device(b, b->moments);
    if (st != VLGPU_OK) return st;
    b->pivot_valid = true;
    return VLGPU_OK;
@@ -293,7 +295,7 @@ int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order) {
       if (st != VLGPU_OK) return st;
    }
    // "_R" moments; their first pass is also the acceleration's pivot record
-   const int st = moments_pair_device(b, b->pivot, b->moments_r);
+   const int st = moments_both_device(b, b->moments_r);
    if (st != VLGPU_OK) return st;
    b->pivot_valid = true;
    // the next step starts with a translation, so its pivot is found anew
@@ -667,11 +669,8 @@ int vlgpu_batch_rho_loss(vlgpu_batch* b, double* out) {
 int vlgpu_batch_moments(vlgpu_batch* b, int compute_second, double* out16) {
    if (!b || !out16) return VLGPU_EINVAL;
    VL_CHECK(cudaSetDevice(b->device));
-   // the second moments are taken about the bulk velocity of the current VDF,
-   // found by a first pass over each cell in the same launch
-   const int st = compute_second ? moments_pair_device(b, b->pivot, b->moments) : moments_device(b, false);
+   const int st = compute_second ? moments_both_device(b, b->moments) : moments_device(b, false);
    if (st != VLGPU_OK) return st;
-   if (compute_second) b->pivot_valid = true;
    VL_CHECK(cudaMemcpyAsync(out16, b->moments, sizeof(double) * MOM_COUNT * b->n_cells, cudaMemcpyDeviceToHost,
                             b->stream));
    VL_CHECK(cudaStreamSynchronize(b->stream));

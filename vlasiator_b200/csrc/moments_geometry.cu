@@ -98,10 +98,9 @@ __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* s
 // One CTA per cell; 16 threads per velocity block, each owning one x-row of
 // four cells (a float4: i = 0..3 at j = sub & 3, k = sub >> 2), and every
 // thread group keeps MOM_UNROLL blocks in flight.  With SECOND, velocities
-// are taken relative to a reference velocity U (a bulk velocity of the same
-// or of the previous VDF of the cell: the first pass of the moments pair, or
-// the acceleration step's pivot), so one pass over the data gives both the
-// first moments and the central second moments:
+// are taken relative to a reference velocity U (a bulk velocity of an
+// earlier VDF of the cell: the acceleration step's pivot), so one pass over
+// the data gives both the first moments and the central second moments:
 //   S0 = sum f, S_a = sum f u_a, S_ab = sum f u_a u_b   (u = v - U)
 //   n V_a = (S_a + U_a S0) dv^3,  P_ab = m dv^3 (S_ab - S_a S_b / S0).
 // With U close to V the correction term is small, so nothing cancels; the
@@ -111,20 +110,37 @@ __device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* s
 //
 // moments_pass is one such pass of a CTA over one cell's blocks; thread 0
 // writes the cell's record `out`.
-template <bool SECOND>
+//
+// MODE MOM_BOTH does the work of a first-moments pass and a second-moments
+// pass in one read: the first sums with U = 0 (the same arithmetic as
+// MOM_FIRST, so the first moments are identical) and the second sums about
+// the U given, whose first sums T_a = S_a - U_a S0 follow from the former;
+// the cancellation in T_a costs about eps (U / v_th)^2 of P relative, far
+// below the tolerance of any use, and vanishes as U approaches V.  It writes
+// the first moments to `out1` (pressure zero, as MOM_FIRST) and everything
+// to `out`.
+constexpr int MOM_FIRST = 0, MOM_SECOND = 1, MOM_BOTH = 2;
+
+template <int MODE>
 __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index,
                                              const float* __restrict__ data, const CellSlot s, double* out,
                                              const MeshDev& mesh, double vmin0, double vmin1, double vmin2, double bs0,
                                              double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
                                              double charge, double U0, double U1, double U2, double* sh_hi,
-                                             double* sh_lo) {
+                                             double* sh_lo, double* out1 = nullptr) {
+   constexpr bool SECOND = MODE != MOM_FIRST;
    constexpr int NS = SECOND ? 10 : 4;
    const int sub = threadIdx.x & 15, grp = threadIdx.x >> 4;
    const int j = sub & 3, k = sub >> 2;
-   const double cy = (j + 0.5) * dv1 - U1, cz = (k + 0.5) * dv2 - U2;
-   const double cx0 = 0.5 * dv0 - U0, cx1 = 1.5 * dv0 - U0, cx2 = 2.5 * dv0 - U0, cx3 = 3.5 * dv0 - U0;
+   // velocity offsets of the first sums (U = 0 in MOM_BOTH) and of the second
+   const double F0 = (MODE == MOM_BOTH) ? 0.0 : U0, F1 = (MODE == MOM_BOTH) ? 0.0 : U1;
+   const double F2 = (MODE == MOM_BOTH) ? 0.0 : U2;
+   const double cy = (j + 0.5) * dv1 - F1, cz = (k + 0.5) * dv2 - F2;
+   const double cx0 = 0.5 * dv0 - F0, cx1 = 1.5 * dv0 - F0, cx2 = 2.5 * dv0 - F0, cx3 = 3.5 * dv0 - F0;
+   const double sy = (j + 0.5) * dv1 - U1, sz = (k + 0.5) * dv2 - U2;
+   const double sx0 = 0.5 * dv0 - U0, sx1 = 1.5 * dv0 - U0, sx2 = 2.5 * dv0 - U0, sx3 = 3.5 * dv0 - U0;
    Kahan acc[NS];
-   constexpr int MOM_UNROLL = SECOND ? 4 : 8;  // blocks in flight per thread group
+   constexpr int MOM_UNROLL = (MODE == MOM_FIRST) ? 8 : (MODE == MOM_SECOND ? 4 : 2);  // blocks in flight per group
    constexpr uint32_t STEP = MOM_GROUPS * MOM_UNROLL;
    // block IDs and data indices of a batch; the next batch's are loaded while
    // the current batch's data is in flight, so a batch waits on one round
@@ -139,6 +155,14 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
       }
    };
    fetch(grp, g, idx);
+   // per-thread sums of a batch, added to the compensated sums once per
+   // batch; in MOM_BOTH the first sums keep MOM_FIRST's batches of 8 blocks
+   // (four of its batches of 2, same blocks in the same order), so that its
+   // first moments are bit-identical to a MOM_FIRST pass
+   double t[NS];
+#pragma unroll
+   for (int q = 0; q < NS; ++q) t[q] = 0.0;
+   int vb = 0;
    for (uint32_t b0 = grp; b0 < s.count; b0 += STEP) {
       float4 f4[MOM_UNROLL];
 #pragma unroll
@@ -149,10 +173,6 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
       }
       uint32_t g_next[MOM_UNROLL], idx_next[MOM_UNROLL];
       fetch(b0 + STEP, g_next, idx_next);
-      // the batch's blocks are summed plainly, the batch sums compensated
-      double t[NS];
-#pragma unroll
-      for (int q = 0; q < NS; ++q) t[q] = 0.0;
 #pragma unroll
       for (int u = 0; u < MOM_UNROLL; ++u) {
          uint32_t bi, bj, bk;
@@ -169,7 +189,7 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
          t[1] += sfx;
          t[2] += sf * uy;
          t[3] += sf * uz;
-         if constexpr (SECOND) {
+         if constexpr (MODE == MOM_SECOND) {
             t[4] += (fx0 * x0 + fx1 * x1) + (fx2 * x2 + fx3 * x3);
             t[5] += sf * uy * uy;
             t[6] += sf * uz * uz;
@@ -177,14 +197,49 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
             t[8] += sfx * uz;
             t[9] += sfx * uy;
          }
+         if constexpr (MODE == MOM_BOTH) {
+            const double vy = (vmin1 + bj * bs1) + sy, vz = (vmin2 + bk * bs2) + sz;
+            const double y0 = bx + sx0, y1 = bx + sx1, y2 = bx + sx2, y3 = bx + sx3;
+            const double fy0 = f0 * y0, fy1 = f1 * y1, fy2 = f2 * y2, fy3 = f3 * y3;
+            const double sfy = (fy0 + fy1) + (fy2 + fy3);
+            t[4] += (fy0 * y0 + fy1 * y1) + (fy2 * y2 + fy3 * y3);
+            t[5] += sf * vy * vy;
+            t[6] += sf * vz * vz;
+            t[7] += sf * vy * vz;
+            t[8] += sfy * vz;
+            t[9] += sfy * vy;
+         }
       }
+      if constexpr (MODE == MOM_BOTH) {
 #pragma unroll
-      for (int q = 0; q < NS; ++q) acc[q].add(t[q]);
+         for (int q = 4; q < NS; ++q) {
+            acc[q].add(t[q]);
+            t[q] = 0.0;
+         }
+         if (++vb == 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+               acc[q].add(t[q]);
+               t[q] = 0.0;
+            }
+            vb = 0;
+         }
+      } else {
+#pragma unroll
+         for (int q = 0; q < NS; ++q) {
+            acc[q].add(t[q]);
+            t[q] = 0.0;
+         }
+      }
 #pragma unroll
       for (int u = 0; u < MOM_UNROLL; ++u) {
          g[u] = g_next[u];
          idx[u] = idx_next[u];
       }
+   }
+   if (MODE == MOM_BOTH && vb) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q].add(t[q]);
    }
    double hi[NS], lo[NS];
 #pragma unroll
@@ -199,7 +254,7 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
    for (int q = 0; q < NS; ++q) S[q] = hi[q] + lo[q];
    const double DV3 = dv0 * dv1 * dv2;
    const double a0 = S[0] * DV3;
-   const double a1 = (S[1] + U0 * S[0]) * DV3, a2 = (S[2] + U1 * S[0]) * DV3, a3 = (S[3] + U2 * S[0]) * DV3;
+   const double a1 = (S[1] + F0 * S[0]) * DV3, a2 = (S[2] + F1 * S[0]) * DV3, a3 = (S[3] + F2 * S[0]) * DV3;
    out[MOM_N] = a0;
    out[MOM_NVX] = a1;
    out[MOM_NVY] = a2;
@@ -214,17 +269,24 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
    double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
    if constexpr (SECOND) {
       if (S[0] != 0.0) {
-         const double m1 = S[1] / S[0], m2 = S[2] / S[0], m3 = S[3] / S[0];
+         // first sums about U (those of MOM_BOTH were taken about 0)
+         const double T1 = (MODE == MOM_BOTH) ? S[1] - U0 * S[0] : S[1];
+         const double T2 = (MODE == MOM_BOTH) ? S[2] - U1 * S[0] : S[2];
+         const double T3 = (MODE == MOM_BOTH) ? S[3] - U2 * S[0] : S[3];
+         const double m1 = T1 / S[0], m2 = T2 / S[0], m3 = T3 / S[0];
          const double pre = mass * DV3;
-         P[0] = pre * (S[4] - S[1] * m1);
-         P[1] = pre * (S[5] - S[2] * m2);
-         P[2] = pre * (S[6] - S[3] * m3);
-         P[3] = pre * (S[7] - S[2] * m3);
-         P[4] = pre * (S[8] - S[1] * m3);
-         P[5] = pre * (S[9] - S[1] * m2);
+         P[0] = pre * (S[4] - T1 * m1);
+         P[1] = pre * (S[5] - T2 * m2);
+         P[2] = pre * (S[6] - T3 * m3);
+         P[3] = pre * (S[7] - T2 * m3);
+         P[4] = pre * (S[8] - T1 * m3);
+         P[5] = pre * (S[9] - T1 * m2);
       }
    }
    for (int q = 0; q < 6; ++q) out[MOM_P11 + q] = P[q];
+   if (MODE == MOM_BOTH && out1) {
+      for (int q = 0; q < MOM_COUNT; ++q) out1[q] = (q >= MOM_P11 && q < MOM_P11 + 6) ? 0.0 : out[q];
+   }
 }
 
 // With SECOND the reference velocity U is the bulk velocity in the cell's
@@ -241,38 +303,8 @@ __global__ void __launch_bounds__(MOM_THREADS, 2) moments_kernel(
    double* out = moments + (size_t)cell * MOM_COUNT;
    const double* sh = shift + (size_t)cell * MOM_COUNT;
    const double U0 = SECOND ? sh[MOM_VX] : 0.0, U1 = SECOND ? sh[MOM_VY] : 0.0, U2 = SECOND ? sh[MOM_VZ] : 0.0;
-   moments_pass<SECOND>(gids, src_index, data, slots[cell], out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1,
-                        dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo);
-}
-
-// Both passes of a cell in one CTA: the first moments (U = 0) into `first`
-// (or into `moments` when first is null), then the second moments about the
-// bulk velocity just found into `moments`.  The same arithmetic as the
-// first-moments launch followed by the second-moments launch, so the records
-// are identical; the second pass reads the cell's blocks again right after
-// the first, mostly from L2.
-__global__ void __launch_bounds__(MOM_THREADS, 2) moments_pair_kernel(
-   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
-   const CellSlot* __restrict__ slots, double* __restrict__ first, double* __restrict__ moments, MeshDev mesh,
-   double vmin0, double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2,
-   double mass, double charge) {
-   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   __shared__ double s_U[3];
-   const uint32_t cell = blockIdx.x;
-   const CellSlot s = slots[cell];
-   double* out = moments + (size_t)cell * MOM_COUNT;
-   double* out1 = first ? first + (size_t)cell * MOM_COUNT : out;
-   moments_pass<false>(gids, src_index, data, s, out1, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
-                       charge, 0.0, 0.0, 0.0, sh_hi, sh_lo);
-   if (threadIdx.x == 0) {
-      s_U[0] = out1[MOM_VX];
-      s_U[1] = out1[MOM_VY];
-      s_U[2] = out1[MOM_VZ];
-   }
-   __syncthreads();
-   moments_pass<true>(gids, src_index, data, s, out, mesh, vmin0, vmin1, vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass,
-                      charge, s_U[0], s_U[1], s_U[2], sh_hi, sh_lo);
+   moments_pass<SECOND ? MOM_SECOND : MOM_FIRST>(gids, src_index, data, slots[cell], out, mesh, vmin0, vmin1, vmin2,
+                                                 bs0, bs1, bs2, dv0, dv1, dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo);
 }
 
 // Per-cell acceleration inputs on the device.
@@ -401,12 +433,30 @@ cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, cons
    return cudaGetLastError();
 }
 
-cudaError_t launch_moments_pair(const uint32_t* gids, const uint32_t* src_index, const float* data,
-                                const CellSlot* slots, double* first, double* moments, const MeshDev& mesh,
+// MOM_BOTH of every cell: reference velocity U from the cell's record in
+// `pivot`, which then receives the first moments of this VDF; the moments
+// with pressure go to `moments`.
+__global__ void __launch_bounds__(MOM_THREADS, 2) moments_both_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
+   const CellSlot* __restrict__ slots, double* pivot, double* __restrict__ moments, MeshDev mesh, double vmin0,
+   double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
+   double charge) {
+   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
+   const uint32_t cell = blockIdx.x;
+   double* pv = pivot + (size_t)cell * MOM_COUNT;
+   const double U0 = pv[MOM_VX], U1 = pv[MOM_VY], U2 = pv[MOM_VZ];
+   __syncthreads();  // every thread has read U before thread 0 overwrites the record
+   moments_pass<MOM_BOTH>(gids, src_index, data, slots[cell], moments + (size_t)cell * MOM_COUNT, mesh, vmin0, vmin1,
+                          vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo, pv);
+}
+
+cudaError_t launch_moments_both(const uint32_t* gids, const uint32_t* src_index, const float* data,
+                                const CellSlot* slots, double* pivot, double* moments, const MeshDev& mesh,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
                                 double charge, uint32_t n_cells, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
-   moments_pair_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, first, moments, mesh,
+   moments_both_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, pivot, moments, mesh,
                                                            vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
                                                            dv[1], dv[2], mass, charge);
    return cudaGetLastError();
