@@ -10,9 +10,15 @@ FP64 gyration geometry, three 1D remaps in a random dimension order) with
 dt = 0.01 gyroperiod per cell.
 
 Metric: phase-space cell-updates/s, one update = one of the 64 cells of a
-block existing before the step advanced through the three sweeps.
+block existing before the step advanced through the three sweeps.  `value`
+is device time with the batch resident in HBM; `e2e` runs the same step
+through the C ABI from pinned host buffers, the cells split into 32 batches
+whose uploads, steps and downloads overlap; `cpu_baseline` and
+`--impl reference` time the reference's own map_1d built from its sources.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload vlasov     # full Vlasov step, 64x64x16 sine-wave grid
+    python bench.py --workload serve      # Poisson stream of requests
 
 Prints one JSON line (rank 0).  Under torchrun each rank runs its own batch
 (independent cells, weak scaling, no collective on the data path).
