@@ -34,3 +34,33 @@ def test_library_exports_all_declared_symbols():
 
 def test_version_string():
     assert b"sm_100a" in vlgpu.load().vlgpu_version()
+
+
+def test_header_compiles_as_c99_and_links(tmp_path):
+    """include/vlgpu.h is plain C: a C99 caller of the batch life cycle and of
+    the asynchronous pipeline compiles without warnings and links against the
+    library (nothing is run)."""
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdint.h>
+#include "vlgpu.h"
+int step(vlgpu_batch* b, const uint64_t* offs, const uint32_t* gids, const float* data,
+         const vlgpu_cell_fields* fields, const double* dt, uint32_t* off, uint32_t* cnt,
+         uint32_t* out_g, float* out_d, uint64_t cap) {
+   uint64_t used = 0;
+   int st = vlgpu_batch_upload_async(b, offs, gids, data);
+   if (st == VLGPU_OK) st = vlgpu_accelerate(b, fields, dt, 0);
+   if (st == VLGPU_OK) st = vlgpu_batch_download_begin(b);
+   if (st == VLGPU_OK) st = vlgpu_batch_download_end(b, off, cnt, out_g, out_d, cap, &used);
+   if (st == VLGPU_OK) st = vlgpu_batch_sync(b);
+   return st;
+}
+int main(void) { return vlgpu_version() == 0; }
+''')
+    from vlasiator_b200.build import build
+    build()
+    lib_dir = os.path.dirname(vlgpu.LIB_PATH)
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-L", lib_dir, "-lvlgpu", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
