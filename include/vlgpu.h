@@ -124,12 +124,13 @@ int vlgpu_map_1d(vlgpu_batch* b, const double* intersections, uint32_t dimension
    drop-in path, vlasovsolver/cpu_acc_semilag.cpp:64-75 without OpenMP). */
 int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t dimension);
 
-/* The same sweep (with the default fused remap arithmetic, see
-   vlgpu_batch_set_exact) for callers that must not allocate device memory.  It has no
-   counterpart in the reference: it exists for host codes that reserve all of
-   the GPU's memory for their own pool at start-up, and for codes that call
-   the sweep on a latency-critical path, where a cudaMalloc/cudaFree would
-   synchronise the whole device.  It allocates nothing: its work arrays live
+/* The same sweep for callers that must not allocate device memory.  It
+   always runs the fused arithmetic with PPM (the defaults of a batch, see
+   vlgpu_batch_set_exact and vlgpu_batch_set_reconstruction), whatever mode a
+   batch would use.  It has no counterpart in the reference: it exists for
+   host codes that reserve all of the GPU's memory for their own pool at
+   start-up, and for codes that call the sweep on a latency-critical path,
+   where a cudaMalloc/cudaFree would synchronise the whole device.  It allocates nothing: its work arrays live
    in one fixed device array of about 3.3 MB inside libvlgpu.so, held by every
    GPU that loads the library until the process exits.
    Limits per call: 1..VLGPU_NOALLOC_MAX_CELLS cells, input block indices
@@ -144,11 +145,14 @@ int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t 
    blocks are cell_off[c] .. cell_off[c]+cell_count[c]-1 of them, in sweep
    order (host arrays of n_cells); status (host, may be NULL) gets each cell's
    VLGPU_CELL_* bits of this call.  data_in and data_out are 16-byte aligned.
+   The output buffers must not overlap the input buffers (the sweep reads
+   blocks of one cell after writing blocks of another); passing the same
+   pointer for both is rejected with VLGPU_EINVAL.
    The work is issued on `stream` (a cudaStream_t of the current device, NULL
    for the default stream) and the call synchronises it before returning.
-   The first call on a device, with that device current, looks up the device
-   array's address (cudaGetSymbolAddress); make that first call before any
-   stream capture begins.  Every call on a device uses the same array: calls
+   Every call looks up the device array's address (cudaGetSymbolAddress) on
+   the current device; the first call on a device also loads the library's
+   kernels there, so make that first call before any stream capture begins.  Every call on a device uses the same array: calls
    that overlap on the GPU (from several host threads at once) race and must
    be serialised by the caller. */
 #define VLGPU_NOALLOC_MAX_BLOCKS 65536u

@@ -10,10 +10,10 @@
 #   oracle/_ref/libvlasov_ref_dp.so  : all-FP64 (Realf=double), VECL=8, PPM
 #   oracle/_ref/libvlasov_ref_sp_pqm.so, libvlasov_ref_sp_plm.so : FP32, PQM / PLM acceleration
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]   (default $VLASIATOR_REF, else /root/reference)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${VLASIATOR_REF:-/root/reference}}"
 OUT="$HERE/_ref"
 SRC="$OUT/src"
 if [ ! -f "$REF/vlasovsolver/cpu_acc_map.cpp" ]; then
@@ -41,6 +41,19 @@ done
 # copy_trans_block_data_amr, trans_map_1d_amr; lines 1-443), without the MPI
 # remote-contribution functions that follow
 sed -n '1,443p' "$REF/vlasovsolver/cpu_trans_map_amr.cpp" > "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp"
+# block adjustment: the content test and block add/remove of SpatialCell
+# (adjust_velocity_blocks, compute_block_has_content,
+# update_velocity_block_content_lists, updateSparseMinValue; spatial_cell_cpu.cpp
+# lines 179-273, 290-316, 675-688, 699-727) and the grid-level drivers of
+# block_adjust_cpu.cpp (lines 28-119), compiled as members of the stand-in cell
+{
+  printf '#include <iostream>\n#include <unordered_set>\n#include <vector>\n'
+  printf '#include "spatial_cells/spatial_cell_wrapper.hpp"\n#include "object_wrapper.h"\n'
+  printf 'using namespace std;\nnamespace spatial_cell {\n'
+  sed -n '179,273p;290,316p;675,688p;699,727p' "$REF/spatial_cells/spatial_cell_cpu.cpp"
+  printf '}  // namespace spatial_cell\n'
+  sed -n '28,119p' "$REF/spatial_cells/block_adjust_cpu.cpp"
+} > "$SRC/spatial_cells/block_adjust_part.cpp"
 cp "$HERE/ref_shim/grid.h" "$SRC/grid.h"
 cp "$HERE/ref_shim/object_wrapper.h" "$SRC/object_wrapper.h"
 cp "$HERE/ref_shim/spatial_cells/spatial_cell_wrapper.hpp" "$SRC/spatial_cells/spatial_cell_wrapper.hpp"
@@ -53,21 +66,26 @@ COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
         -I"$SRC" -I"$SRC/sysinc" -w)
 SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
       "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
-      "$SRC/velocity_mesh_parameters.cpp" "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp")
+      "$SRC/velocity_mesh_parameters.cpp" "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp"
+      "$SRC/spatial_cells/block_adjust_part.cpp")
 # the oracle's own FP64 geometry restatement (the reference's needs Eigen)
 CC="${REF_CC:-/usr/bin/gcc}"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_sp.o"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -DORC_DOUBLE -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_dp.o"
+rm -f "$OUT"/libvlasov_ref_*.so
+pids=()
 "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PPM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
-  -o "$OUT/libvlasov_ref_sp.so" &
+  -o "$OUT/libvlasov_ref_sp.so" & pids+=($!)
 "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PPM -DDPF -DVECL=8 "${SRCS[@]}" "$OUT/orc_geometry_dp.o" \
-  -o "$OUT/libvlasov_ref_dp.so" &
+  -o "$OUT/libvlasov_ref_dp.so" & pids+=($!)
 # the other acceleration reconstructions of the reference (PQM is its
 # Makefile default, PLM the lowest order), FP32 VDF
 "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PQM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
-  -o "$OUT/libvlasov_ref_sp_pqm.so" &
+  -o "$OUT/libvlasov_ref_sp_pqm.so" & pids+=($!)
 "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PLM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
-  -o "$OUT/libvlasov_ref_sp_plm.so" &
-wait
+  -o "$OUT/libvlasov_ref_sp_plm.so" & pids+=($!)
+fail=0
+for p in "${pids[@]}"; do wait "$p" || fail=1; done
+if [ "$fail" -ne 0 ]; then echo "build_ref: a compilation failed" >&2; exit 4; fi
 for f in sp dp sp_pqm sp_plm; do test -f "$OUT/libvlasov_ref_$f.so"; done
 echo "build_ref: built $OUT/libvlasov_ref_{sp,dp,sp_pqm,sp_plm}.so"

@@ -31,11 +31,17 @@ def _ptr(a, t):
     return a.ctypes.data_as(ctypes.POINTER(t))
 
 
+def reference_root() -> str:
+    """The Vlasiator source tree the reference build reads: $VLASIATOR_REF, else /root/reference."""
+    return os.environ.get("VLASIATOR_REF", "/root/reference")
+
+
 def build(with_reference: bool = False) -> None:
     """Compiles the restatement (and, if asked and available, the reference build)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if with_reference and os.path.isdir("/root/reference/vlasovsolver"):
-        subprocess.run([os.path.join(HERE, "build_ref.sh")], check=True, stdout=subprocess.DEVNULL)
+    ref = reference_root()
+    if with_reference and os.path.isdir(os.path.join(ref, "vlasovsolver")):
+        subprocess.run([os.path.join(HERE, "build_ref.sh"), ref], check=True, stdout=subprocess.DEVNULL)
 
 
 class Restatement:
@@ -278,6 +284,10 @@ class ReferenceBuild:
         L.ref_max_threads.restype = ctypes.c_int
         L.ref_cells_translate.argtypes = [_vp, _u32p, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_int]
+        L.ref_cells_adjust.argtypes = [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_cells_content.restype = ctypes.c_uint64
+        L.ref_cells_content.argtypes = [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64]
 
     def init(self, mesh: VelocityMesh, wall_margin: int = 1):
         vmin = np.array(mesh.vmin, np.float64)
@@ -337,6 +347,28 @@ class ReferenceBuild:
         self.lib.ref_cells_moments(h, c, _ptr(bv, ctypes.c_double), _ptr(f, ctypes.c_double),
                                    _ptr(s, ctypes.c_double))
         return f, s
+
+    def adjust(self, h, n_cells, min_value, add_width=1, neighbors=None, conserve_mass=False, nthreads=0):
+        """adjustVelocityBlocks (grid.cpp:775-817) with the reference's own
+        content lists and adjust_velocity_blocks on every cell of the set;
+        neighbors: (n_cells, k) cell indices (-1: none) or None.  Returns the
+        RHOLOSSADJUST each cell gained."""
+        loss = np.zeros(n_cells)
+        if neighbors is None:
+            nb, k = None, 0
+        else:
+            nbr = np.ascontiguousarray(neighbors, np.int32)
+            nb, k = _ptr(nbr, ctypes.c_int32), nbr.shape[1]
+        self.lib.ref_cells_adjust(h, nb, k, float(min_value), int(add_width), int(conserve_mass), nthreads,
+                                  _ptr(loss, ctypes.c_double))
+        return loss
+
+    def content(self, h, c):
+        """compute_block_has_content of cell c's blocks, in local-ID order."""
+        n = self.lib.ref_cells_block_count(h, c)
+        f = np.zeros(max(n, 1), np.uint8)
+        self.lib.ref_cells_content(h, c, _ptr(f, ctypes.c_uint8), n)
+        return f[:n].astype(bool)
 
     def bailouts(self) -> int:
         return self.lib.ref_bailouts()

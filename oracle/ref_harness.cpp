@@ -1,4 +1,4 @@
-// C entry points over the reference's own CPU acceleration code, used as the
+// C entry points over the reference's own CPU hot-path code, used as the
 // parity oracle and CPU baseline (test infrastructure only; built by
 // oracle/build_ref.sh into oracle/_ref/, never linked into the product).
 //
@@ -20,6 +20,14 @@
 #include "vlasovsolver/arch_moments.h"
 #include "vlasovsolver/cpu_trans_map_amr.hpp"
 #include "vlasovsolver/cpu_trans_pencils.hpp"
+
+namespace spatial_cell {
+// the reference's grid-level block adjustment (spatial_cells/block_adjust_cpu.cpp:33-117)
+void update_velocity_block_content_lists(dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry>& mpiGrid,
+                                         const std::vector<CellID>& cells, const uint popID);
+void adjust_velocity_blocks_in_cells(dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry>& mpiGrid,
+                                     const std::vector<CellID>& cellsToAdjust, const uint popID);
+}  // namespace spatial_cell
 
 using spatial_cell::SpatialCell;
 
@@ -90,7 +98,7 @@ void* ref_cells_create(uint32_t n_cells, const uint64_t* offsets, const uint32_t
    for (uint32_t c = 0; c < n_cells; ++c) {
       SpatialCell* sc = new SpatialCell(1);
       sc->get_velocity_mesh(0)->initialize(0);
-      sc->populations[0]->velocityBlockMinValue = min_values[c];
+      sc->populations[0].velocityBlockMinValue = min_values[c];
       sc->parameters[CellParams::CELLID] = c + 1;
       const uint64_t b0 = offsets[c], b1 = offsets[c + 1];
       for (uint64_t b = b0; b < b1; ++b) {
@@ -216,6 +224,56 @@ void ref_cells_accelerate_step(void* h, const double* B, const double* dt, uint3
          map_1d(sc, 0, I[4 * d + 0], I[4 * d + 1], I[4 * d + 2], I[4 * d + 3], d);
       }
    }
+}
+
+// Block adjustment of every cell of the set as adjustVelocityBlocks does it
+// (grid.cpp:775-817): the reference's own update_velocity_block_content_lists
+// (block_adjust_cpu.cpp:33-53, with updateSparseMinValue and
+// compute_block_has_content, spatial_cell_cpu.cpp:290-316, 675-727) for all
+// cells first, then adjust_velocity_blocks_in_cells (block_adjust_cpu.cpp:
+// 55-117) calling SpatialCell::adjust_velocity_blocks (spatial_cell_cpu.cpp:
+// 179-273).  Cell c has dccrg id c+1; neighbors holds n_per_cell cell indices
+// per cell (-1: none) -- the cell's NEAREST neighbourhood -- or is null (no
+// spatial neighbours).  The species' minValue and blockAddWidthV are set from
+// min_value and add_width; rho_loss gets each cell's RHOLOSSADJUST added by
+// this call.
+void ref_cells_adjust(void* h, const int32_t* neighbors, uint32_t n_per_cell, double min_value, int add_width,
+                      int conserve_mass, int nthreads, double* rho_loss) {
+   RefCells* rc = (RefCells*)h;
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+   species::Species& sp = getObjectWrapper().particleSpecies[0];
+   sp.sparseMinValue = min_value;
+   sp.sparseBlockAddWidthV = add_width;
+   sp.sparse_conserve_mass = conserve_mass != 0;
+   sp.sparseDynamicAlgorithm = 0;
+   dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry> g;
+   std::vector<CellID> cells;
+   std::vector<double> before(rc->cells.size());
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      g.cells[c + 1] = rc->cells[c];
+      cells.push_back(c + 1);
+      before[c] = rc->cells[c]->populations[0].RHOLOSSADJUST;
+      if (neighbors) {
+         auto& list = g.neighbor_lists[c + 1];
+         for (uint32_t q = 0; q < n_per_cell; ++q) {
+            const int32_t n = neighbors[(size_t)c * n_per_cell + q];
+            if (n >= 0) list.push_back({(uint64_t)n + 1, std::array<int, 4>{0, 0, 0, 0}});
+         }
+      }
+   }
+   spatial_cell::update_velocity_block_content_lists(g, cells, 0);
+   spatial_cell::adjust_velocity_blocks_in_cells(g, cells, 0);
+   for (size_t c = 0; c < rc->cells.size(); ++c) rho_loss[c] = rc->cells[c]->populations[0].RHOLOSSADJUST - before[c];
+}
+
+// The content flag of every block of cell c in local-ID order, as the
+// reference's compute_block_has_content gives it (spatial_cell_cpu.cpp:290-316).
+uint64_t ref_cells_content(void* h, uint32_t c, uint8_t* flags, uint64_t cap) {
+   SpatialCell* sc = ((RefCells*)h)->cells[c];
+   const uint64_t n = sc->get_velocity_mesh(0)->size();
+   if (n > cap) return n;
+   for (uint64_t lid = 0; lid < n; ++lid) flags[lid] = sc->compute_block_has_content((vmesh::LocalID)lid, 0) ? 1 : 0;
+   return n;
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }

@@ -1,8 +1,9 @@
 // Minimal stand-in for the reference's object_wrapper.h, used only when the
 // reference's own hot-path sources are compiled as the parity oracle
 // (oracle/build_ref.sh).  It provides the two things those sources touch:
-// particle species metadata (name, mass, charge, sparsity settings) and the
-// Parameters struct members read on the acceleration path.
+// particle species metadata (name, mass, charge, sparsity settings, as
+// particle_species.h names them) and the Parameters struct members read on
+// the acceleration path.
 #pragma once
 #include <string>
 #include <vector>
@@ -17,6 +18,10 @@ struct Species {
    int sparseBlockAddWidthV{1};
    bool sparse_conserve_mass{false};
    int sparseDynamicAlgorithm{0};
+   Real sparseDynamicBulkValue1{0};
+   Real sparseDynamicBulkValue2{0};
+   Real sparseDynamicMinValue1{0};
+   Real sparseDynamicMinValue2{0};
 };
 }  // namespace species
 

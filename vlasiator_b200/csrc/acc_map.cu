@@ -9,21 +9,22 @@
 //                     the cell's output blocks and writes one ColumnSet record
 //                     per transverse pair plus the source permutation.
 //
-//   remap_kernel      persistent; each half-warp takes one ColumnSet and
-//                     walks it along the sweep dimension, one lane per
-//                     transverse cell (i,j) of the 4x4 block face.  PPM
-//                     coefficients are built in registers from a sliding
-//                     5-cell window; each source cell's mass is distributed
-//                     over the Lagrangian target cells it overlaps into a
-//                     per-lane ring of 8 target blocks in shared memory, and
-//                     completed target blocks are streamed out.  Every output
-//                     block is written exactly once, so no zero fill and no
-//                     atomics are needed.
+//   remap_walk_kernel (the default, fused arithmetic) or remap_kernel (the
+//                     exact mode): persistent; each half-warp takes one
+//                     ColumnSet and walks it along the sweep dimension, one
+//                     lane per transverse cell (i,j) of the 4x4 block face.
+//                     The reconstruction is built in registers from a sliding
+//                     window of the column; each source cell's mass goes to
+//                     the Lagrangian target cells it overlaps in a per-lane
+//                     ring of 8 target blocks in shared memory, and completed
+//                     target blocks are streamed out.  Every output block is
+//                     written exactly once, so no zero fill and no atomics are
+//                     needed.
 //
-// Arithmetic follows the reference's scalar build operation by operation
-// (round-to-nearest intrinsics, no contraction, the double-precision
-// products of cpu_face_estimates.hpp:163 and cpu_acc_map.cpp:585), so results
-// are bit-identical to the reference's map_1d on the same inputs.
+// remap_kernel follows the reference's scalar build operation by operation
+// (round-to-nearest intrinsics, no contraction, the double-precision products
+// of cpu_face_estimates.hpp:163 and cpu_acc_map.cpp:585), so its results are
+// bit-identical to the reference's map_1d on the same inputs.
 #include <cfloat>
 #include <cstdint>
 
@@ -48,10 +49,6 @@ __device__ __forceinline__ float h4_face(float vm2, float vm1, float v0, float v
    s = fa(s, fm(7.0f, v0));
    s = fs(s, vp1);
    return dmf(1.0 / 12.0, s);
-}
-template <bool FUSED>
-__device__ __forceinline__ float h4_face_mode(float vm2, float vm1, float v0, float vp1) {
-   return FUSED ? h4_face_fused(vm2, vm1, v0, vp1) : h4_face(vm2, vm1, v0, vp1);
 }
 
 __device__ __forceinline__ float minmod(float s1, float s2) {
@@ -435,8 +432,8 @@ __device__ __forceinline__ void select_lanes(float lag, int lane, unsigned hmask
    min_lane = vmin ? imin : 0;
 }
 
-template <int DIM, bool EXACT, int RECON>
-__global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) remap_kernel(
+template <int DIM>
+__global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
    const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
    const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
@@ -475,12 +472,6 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
       const float im = fa(fa(P.intersection, fm(A, P.di)), fm(B, P.dj));
       float mx, mn;
       set_corners(P, cs.si, cs.sj, mx, mn);
-      // fused mode: each lane walks the reference's target edges
-      // (g+1)*dk + im along the column instead of dividing per cell, and a
-      // source cell covers at most three target cells, which holds while the
-      // Lagrangian cell is wider than half a source cell
-      const float inv_dv = (float)i_dv;
-      const bool fused = !EXACT && dk > 0.55f * dv;
       int next_flush = mask_next_set(cs.tgt_mask, 0);
       uint32_t out_idx = 0;
       bool range_err = false;
@@ -529,36 +520,9 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          {
             const float lag = fd(fs(v_r, im), dk);
             gk_r = __float2int_rz(lag);
-            if (!fused) select_lanes(lag, lane, hmask, max_lane, min_lane);  // the exact loop's lanes
+            select_lanes(lag, lane, hmask, max_lane, min_lane);
          }
          const int gk_lo_col = cf * WID, gk_hi_col = (cl + 1) * WID - 1;
-         // fused mode: g0 = the lane's first target (edge(g0+1) > v), e1/e2 =
-         // edge(g0+1)/edge(g0+2), gf = g0 as a float; acc0..acc2 hold the
-         // mass of targets g0..g0+2, which pass into the ring as g0 advances
-         int g0 = gk_r - 2;
-         float gf = (float)g0;
-         float e1 = fa(fm(gf + 1.0f, dk), im), e2 = fa(fm(gf + 2.0f, dk), im);
-         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
-         // highest target the ring can take before its next flush; a target
-         // handed over is never below the flushed ones (the flush bound is
-         // the lowest g0 of the half-warp)
-         int win_hi = (next_flush + RING_BLOCKS) * WID - 1;
-         auto evict = [&](float acc, int g) {
-            if (acc != 0.0f) {
-               const int t = clampi(g, gk_lo_col, gk_hi_col);
-               range_err |= t > win_hi;
-               float* r = &ring[(t & (RING_CELLS - 1)) * 16 + lane];
-               *r += acc;
-            }
-         };
-         if (fused) {
-            for (int q = 0; q < 6 && e1 <= v_r; ++q) {
-               ++g0;
-               gf += 1.0f;
-               e1 = e2;
-               e2 = fa(fm(gf + 2.0f, dk), im);
-            }
-         }
          float pw[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // the previous block (zero padding at a column start)
          float cur[4], nxt[4];
          load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
@@ -567,13 +531,8 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          } else {
             nxt[0] = nxt[1] = nxt[2] = nxt[3] = 0.0f;
          }
-         // raw left face of the column's first cell (and its derivative for PQM)
-         float face = 0.0f, face_d = 0.0f;
-         if constexpr (RECON == RECON_PPM) face = h4_face_mode<!EXACT>(pw[2], pw[3], cur[0], cur[1]);
-         if constexpr (RECON == RECON_PQM) {
-            face = h8_value(pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3]);
-            face_d = h7_derivative(pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3]);
-         }
+         // raw left face of the column's first cell
+         float face = h4_face(pw[2], pw[3], cur[0], cur[1]);
          for (int kb = col_s; kb <= col_e; ++kb) {
             float nn[4];
             if (kb + 2 <= col_e) {
@@ -581,68 +540,17 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
             } else {
                nn[0] = nn[1] = nn[2] = nn[3] = 0.0f;
             }
-            // cell g of the block is w[g + 4]; the stencil reaches 4 cells each way
+            // cell g of the block is w[g + 4]; the stencil reaches 2 cells each way
             const float w[12] = {pw[0], pw[1], pw[2], pw[3], cur[0], cur[1], cur[2], cur[3],
                                  nxt[0], nxt[1], nxt[2], nxt[3]};
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
-               float a[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-               if constexpr (RECON == RECON_PPM) {
-                  const float fr = h4_face_mode<!EXACT>(w[g + 3], w[g + 4], w[g + 5], w[g + 6]);
-                  if constexpr (EXACT)
-                     ppm_coeff(w[g + 3], w[g + 4], w[g + 5], face, fr, threshold, scale, a[0], a[1], a[2]);
-                  else
-                     ppm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], face, fr, a[0], a[1], a[2]);
-                  face = fr;
-               } else if constexpr (RECON == RECON_PQM) {
-                  const float fr = h8_value(w[g + 1], w[g + 2], w[g + 3], w[g + 4], w[g + 5], w[g + 6], w[g + 7],
-                                            w[g + 8]);
-                  const float fdr = h7_derivative(w[g + 1], w[g + 2], w[g + 3], w[g + 4], w[g + 5], w[g + 6],
-                                                  w[g + 7], w[g + 8]);
-                  pqm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], face, fr, face_d, fdr, a);
-                  face = fr;
-                  face_d = fdr;
-               } else {
-                  plm_coeff_fused(w[g + 3], w[g + 4], w[g + 5], a);
-               }
+               float a[3];
+               const float fr = h4_face(w[g + 3], w[g + 4], w[g + 5], w[g + 6]);
+               ppm_coeff(w[g + 3], w[g + 4], w[g + 5], face, fr, threshold, scale, a[0], a[1], a[2]);
+               face = fr;
                const float v_l = v_r;
                v_r = fa(v_r, dv);
-               if (fused) {
-                  // first target of this source cell: advance past edges <= v_l
-                  // (at most two, as dk > 0.55 dv), handing finished targets
-                  // to the ring
-                  if (e1 <= v_l) {
-                     evict(acc0, g0);
-                     acc0 = acc1;
-                     acc1 = acc2;
-                     acc2 = 0.0f;
-                     ++g0;
-                     gf += 1.0f;
-                     e1 = e2;
-                     e2 = fa(fm(gf + 2.0f, dk), im);
-                  }
-                  if (e1 <= v_l) {  // a second edge inside the same source cell
-                     evict(acc0, g0);
-                     acc0 = acc1;
-                     acc1 = acc2;
-                     acc2 = 0.0f;
-                     ++g0;
-                     gf += 1.0f;
-                     e1 = e2;
-                     e2 = fa(fm(gf + 2.0f, dk), im);
-                  }
-                  // integrals up to the two edges inside the source cell; if
-                  // e1 lies beyond v_r then so does e2 and D1 = D2 = De
-                  const float u1 = (e1 >= v_r) ? 1.0f : (e1 - v_l) * inv_dv;
-                  const float u2 = (e2 >= v_r) ? 1.0f : (e2 - v_l) * inv_dv;
-                  const float De = recon_integral<RECON>(1.0f, a);
-                  const float D1 = recon_integral<RECON>(u1, a);
-                  const float D2 = recon_integral<RECON>(u2, a);
-                  acc0 += D1;
-                  acc1 += D2 - D1;
-                  acc2 += De - D2;
-                  continue;
-               }
                const int gk_l = gk_r;
                gk_r = __float2int_rz(fd(fs(v_r, im), dk));
                int min_gk = __shfl_sync(hmask, gk_l, min_lane, 16);
@@ -660,31 +568,21 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
                         x = (x < v_r) ? x : v_r;
                         const float u = __double2float_rn(__dmul_rn((double)fs(x, v_l), i_dv));
                         const float dl = dens_r;
-                        if constexpr (EXACT)
-                           dens_r = fm(u, fa(a[0], fm(u, fa(a[1], fm(u, a[2])))));
-                        else
-                           dens_r = recon_integral<RECON>(u, a);
+                        dens_r = fm(u, fa(a[0], fm(u, fa(a[1], fm(u, a[2])))));
                         float* t = &ring[(gk & (RING_CELLS - 1)) * 16 + lane];
                         *t = fa(*t, fs(dens_r, dl));
                      }
                   }
                }
             }
-            if (fused && kb == col_e) {
-               // column done: its last targets go to the ring before the flush
-               evict(acc0, g0);
-               evict(acc1, g0 + 1);
-               evict(acc2, g0 + 2);
-            }
             // targets below the next source cell's lower bound are complete
             int lb = ncf * WID;
             if (kb < col_e) {
-               int nl = fused ? __reduce_min_sync(hmask, g0) : __shfl_sync(hmask, gk_r, min_lane, 16);
+               int nl = __shfl_sync(hmask, gk_r, min_lane, 16);
                nl = (nl > gk_lo_col) ? nl : gk_lo_col;
                lb = (nl < lb) ? nl : lb;
             }
             flush_until(lb >> 2);
-            win_hi = (next_flush + RING_BLOCKS) * WID - 1;
 #pragma unroll
             for (int g = 0; g < 4; ++g) {
                pw[g] = cur[g];
@@ -705,6 +603,295 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
          // reads: clear the ring so that the next set starts empty
 #pragma unroll
          for (int q = 0; q < RING_CELLS; ++q) ring[q * 16 + lane] = 0.0f;
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------
+// remap_walk: the fused arithmetic as a single-accumulator walk
+// ---------------------------------------------------------------------------
+// The same column sets, lanes, ring and flushes as remap_kernel, with the
+// reconstruction and the distribution of mass over the target cells reduced
+// to what the fused mode needs:
+//
+//  - PPM: each face's raw h4 value and its test "face outside the values of
+//    the two cells it separates" are evaluated once and used by both cells
+//    (the test of the left face of cell k, (v_{k-1} - f)(f - v_k) < 0, is the
+//    test of the right face of cell k-1 with the same rounded product); the two
+//    Colella-Woodward overshoot corrections are applied as alternatives (in
+//    exact arithmetic the second can no longer fire once the first has).
+//  - Distribution: each lane keeps one pending target g (the lowest target
+//    cell not yet complete), its accumulated mass and the position u of the
+//    target's right edge (g+1) dk + im relative to the current source cell,
+//    in units of dv.  A source cell with the edge inside (u < 1) completes
+//    target g with the integral up to the edge and starts target g+1 with the
+//    rest of the cell (v0 - D(u), so the cell's mass is kept exactly as a
+//    sum); otherwise the whole cell goes to target g.  A second edge inside
+//    one source cell (dk < dv) takes a rare loop.
+//  - Ring traffic: a completed target is stored once into the lane's ring
+//    slot.  Within a column a lane completes each target cell once, and the
+//    targets of different columns of a set never share a cell while dk < 4 dv
+//    (a target would have to span the empty block between them); the first
+//    target of a column starts from what its slot already holds (the last
+//    target of the column before it, when dk >= 4 dv), so targets shared by
+//    two columns are summed in every case.  A flush zeroes the slots it reads.
+//  - Target limits of the column (cpu_acc_map.cpp:559-569): a lane whose first
+//    target lies below the column's lowest target cell starts at that cell,
+//    which then receives all mass below its right edge, as in the reference;
+//    mass of targets above the column's highest cell is moved into it when
+//    the column ends.
+template <int DIM, int RECON>
+__global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) remap_walk_kernel(
+   const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
+   const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
+   const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
+   uint32_t set_capacity, uint8_t* __restrict__ content_out, double content_threshold) {
+   __shared__ float ring_all[(REMAP_THREADS / 16) * RING_STRIDE];
+   const int hw = threadIdx.x >> 4;
+   const int lane = threadIdx.x & 15;
+   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+   float* ring = ring_all + hw * RING_STRIDE + lane;  // this lane's slots: ring[16 * t]
+   const int i = lane & 3, j = lane >> 2;
+   uint32_t n_sets = *((volatile uint32_t*)&counters->n_sets);
+   n_sets = (n_sets < set_capacity) ? n_sets : set_capacity;
+   const int max_len = (int)mesh.len[DIM];
+   const float dv = mesh.dv[DIM], v_min = mesh.vmin[DIM];
+   const float inv_dv = (float)(1.0 / (double)dv);
+   const float content_thr = __double2float_ru(content_threshold);
+   constexpr float one_sixth = (float)(1.0 / 6.0);
+   constexpr int RMASK = RING_CELLS - 1;
+   constexpr uint32_t SMASK = RING_CELLS * 16 - 1;  // slot offsets wrap around the ring
+
+#pragma unroll
+   for (int q = 0; q < RING_CELLS; ++q) ring[q * 16] = 0.0f;
+   for (;;) {
+      uint32_t sidx = 0;
+      if (lane == 0) sidx = atomicAdd(&counters->work, 1u);
+      sidx = __shfl_sync(hmask, sidx, 0, 16);
+      if (sidx >= n_sets) break;
+      const ColumnSet cs = sets[sidx];
+      const SweepCell P = sweep_cells[cs.cell];
+      const float dk = P.dk;
+      const float A = fa((float)(cs.si * WID), (float)i);
+      const float B = fa((float)(cs.sj * WID), (float)j);
+      const float im = fa(fa(P.intersection, fm(A, P.di)), fm(B, P.dj));
+      float mx, mn;
+      set_corners(P, cs.si, cs.sj, mx, mn);
+      const uint32_t gid0 = gid_from_swapped(cs.si, cs.sj, 0u, mesh.len, DIM);
+      const uint32_t gid_step = gid_from_swapped(cs.si, cs.sj, 1u, mesh.len, DIM) - gid0;
+      // the next target block to write and the end of the run of consecutive
+      // target blocks it belongs to
+      int next_flush = mask_next_set(cs.tgt_mask, 0);
+      int run_end = mask_next_clear(cs.tgt_mask, next_flush);
+      uint32_t out_idx = 0;
+      bool range_err = false;
+
+      auto flush_until = [&](int limit_block) {
+         while (next_flush < 96 && next_flush < limit_block) {
+            float v[4];
+            const int slot = (next_flush & (RING_BLOCKS - 1)) * WID;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+               v[g] = ring[(slot + g) * 16];
+               ring[(slot + g) * 16] = 0.0f;
+            }
+            const uint32_t o = cs.dst_pos + out_idx;
+            store_lane<DIM>(dst_data + (size_t)o * WID3, i, j, v);
+            const bool c = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3])) >= content_thr;
+            const unsigned any_c = __ballot_sync(hmask, c) & hmask;
+            if (lane == 0) {
+               dst_gids[o] = gid0 + (uint32_t)next_flush * gid_step;
+               content_out[o] = any_c ? 1 : 0;
+            }
+            ++out_idx;
+            if (++next_flush >= run_end) {
+               next_flush = mask_next_set(cs.tgt_mask, next_flush);
+               run_end = mask_next_clear(cs.tgt_mask, next_flush);
+            }
+         }
+      };
+
+      // a cell whose Lagrangian cells do not advance (flagged by columnize)
+      // gets its target blocks with zero values
+      const bool walkable = dk > 0.0f;
+      int src_rank = 0;
+      int col_s = walkable ? mask_next_set(cs.src_mask, 0) : 96;
+      int col_e = (col_s < 96) ? mask_next_clear(cs.src_mask, col_s) - 1 : 95;
+      int cf = 0, cl = 0;
+      if (col_s < 96) column_extent(mx, mn, dk, dv, v_min, max_len, col_s, col_e, wall_margin, cf, cl);
+      while (col_s < 96) {
+         const int nxt_s = mask_next_set(cs.src_mask, col_e + 1);
+         int nxt_e = 95, ncf = 1 << 20, ncl = 0;
+         if (nxt_s < 96) {
+            nxt_e = mask_next_clear(cs.src_mask, nxt_s) - 1;
+            column_extent(mx, mn, dk, dv, v_min, max_len, nxt_s, nxt_e, wall_margin, ncf, ncl);
+         }
+         const int lo = cf * WID, hi = (cl + 1) * WID - 1;
+         // ---- the lane's first target: the lowest g with (g+1) dk + im > v_l ----
+         float v_l = fa(fm((float)(WID * col_s), dv), v_min);
+         int g = __float2int_rz(fd(fs(v_l, im), dk));
+         float e = fa(fm((float)(g + 1), dk), im);
+         for (int q = 0; q < 3 && e <= v_l; ++q) {
+            ++g;
+            e = fa(fm((float)(g + 1), dk), im);
+         }
+         for (int q = 0; q < 3; ++q) {
+            const float ep = fa(fm((float)g, dk), im);
+            if (!(ep > v_l)) break;
+            --g;
+            e = ep;
+         }
+         if (g < lo) {
+            g = lo;
+            e = fa(fm((float)(g + 1), dk), im);
+         }
+         float g1f = (float)(g + 1);   // the pending target's edge index (g + 1)
+         uint32_t soff = (uint32_t)(g & RMASK) * 16u;  // the pending target's slot
+         float u = fs(e, v_l) * inv_dv;
+         float acc = ring[soff];  // what another column left in the slot
+         float pw0 = 0.0f, pw1 = 0.0f, pw2 = 0.0f, pw3 = 0.0f;  // cells below the block (zero padding)
+         float cur[4], nxt[4];
+         load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
+         if (col_e > col_s) {
+            load_lane<DIM>(src_data, perm[cs.src_pos + src_rank + 1], i, j, nxt);
+         } else {
+            nxt[0] = nxt[1] = nxt[2] = nxt[3] = 0.0f;
+         }
+         // face state of the column's first cell
+         float face = 0.0f, face_d = 0.0f;
+         bool face_out = false;  // PPM: the left face lies outside its two cells' values
+         float dprev = cur[0];   // v_k - v_{k-1}
+         if constexpr (RECON == RECON_PPM) {
+            face = h4_face_fused(0.0f, 0.0f, cur[0], cur[1]);
+            face_out = (0.0f - face) * (face - cur[0]) < 0.0f;
+         }
+         if constexpr (RECON == RECON_PQM) {
+            face = h8_value(0.0f, 0.0f, 0.0f, 0.0f, cur[0], cur[1], cur[2], cur[3]);
+            face_d = h7_derivative(0.0f, 0.0f, 0.0f, 0.0f, cur[0], cur[1], cur[2], cur[3]);
+         }
+         for (int kb = col_s; kb <= col_e; ++kb) {
+            float nn[4];
+            if (kb + 2 <= col_e) {
+               load_lane<DIM>(src_data, perm[cs.src_pos + src_rank + 2], i, j, nn);
+            } else {
+               nn[0] = nn[1] = nn[2] = nn[3] = 0.0f;
+            }
+            const float w[12] = {pw0, pw1, pw2, pw3, cur[0], cur[1], cur[2], cur[3], nxt[0], nxt[1], nxt[2], nxt[3]};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+               const float vm1 = w[q + 3], v0 = w[q + 4], vp1 = w[q + 5];
+               float a[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+               if constexpr (RECON == RECON_PPM) {
+                  const float fr = h4_face_fused(vm1, v0, vp1, w[q + 6]);
+                  const bool fr_out = (v0 - fr) * (fr - vp1) < 0.0f;
+                  const float dn = vp1 - v0;
+                  const bool same = dn * dprev > 0.0f;
+                  // superbee: max(min(|a|, 2|b|), min(2|a|, |b|)) = min(2 min(|a|,|b|), max(|a|,|b|))
+                  const float an = fabsf(dn), ap = fabsf(dprev);
+                  const float sl = fminf(2.0f * fminf(an, ap), fmaxf(an, ap));
+                  const float hs = copysignf(0.5f * sl, dn);
+                  float fl2 = face_out ? v0 - hs : face;
+                  float fr2 = fr_out ? v0 + hs : fr;
+                  fl2 = same ? fl2 : v0;
+                  fr2 = same ? fr2 : v0;
+                  const float d = fr2 - fl2;
+                  const float ev = fmaf(-0.5f, fl2 + fr2, v0);
+                  const float de = d * ev, dd = d * (d * one_sixth);
+                  const float v3 = 3.0f * v0;
+                  const float nfl = (de > dd) ? fmaf(-2.0f, fr2, v3) : fl2;
+                  const float nfr = (-dd > de) ? fmaf(-2.0f, fl2, v3) : fr2;
+                  a[0] = nfl;
+                  a[1] = fmaf(-2.0f, nfl, v3) - nfr;
+                  a[2] = fmaf(-2.0f, v0, nfl + nfr);
+                  face = fr;
+                  face_out = fr_out;
+                  dprev = dn;
+               } else if constexpr (RECON == RECON_PQM) {
+                  const float fr = h8_value(w[q + 1], w[q + 2], w[q + 3], w[q + 4], w[q + 5], w[q + 6], w[q + 7],
+                                            w[q + 8]);
+                  const float fdr = h7_derivative(w[q + 1], w[q + 2], w[q + 3], w[q + 4], w[q + 5], w[q + 6],
+                                                  w[q + 7], w[q + 8]);
+                  pqm_coeff_fused(vm1, v0, vp1, face, fr, face_d, fdr, a);
+                  face = fr;
+                  face_d = fdr;
+               } else {
+                  plm_coeff_fused(vm1, v0, vp1, a);
+               }
+               // ---- distribute the cell over the lane's targets ----
+               const bool has = u < 1.0f;  // the pending target's right edge lies inside this cell
+               float D = recon_integral<RECON>(u, a);  // used only when has
+               if (has) ring[soff] = acc + D;
+               acc = has ? v0 - D : acc + v0;
+               {
+                  const float g1n = g1f + 1.0f;
+                  const float un = fs(fa(fm(g1n, dk), im), v_l) * inv_dv;  // the next edge (reference's rounding)
+                  g1f = has ? g1n : g1f;
+                  u = has ? un : u;
+                  soff = has ? ((soff + 16u) & SMASK) : soff;
+               }
+               if (u < 1.0f) {
+                  // further edges inside the same source cell (dk < dv)
+                  for (int guard = 0; u < 1.0f && guard < 8; ++guard) {
+                     const float D2 = recon_integral<RECON>(u, a);
+                     ring[soff] = D2 - D;
+                     D = D2;
+                     g1f += 1.0f;
+                     soff = (soff + 16u) & SMASK;
+                     u = fs(fa(fm(g1f, dk), im), v_l) * inv_dv;
+                  }
+                  acc = v0 - D;
+               }
+               u -= 1.0f;
+               v_l = fa(v_l, dv);
+            }
+            g = __float2int_rn(g1f) - 1;  // the pending target
+            int top = g - 1;  // the highest target this block completed
+            if (kb == col_e) {
+               // column done: the pending target keeps the rest; targets
+               // above the column's highest cell are folded into it
+               if (g > hi) {
+                  float extra = acc;
+                  for (int t = hi + 1; t < g && t <= hi + RING_CELLS / 2; ++t) {
+                     extra += ring[(t & RMASK) * 16];
+                     ring[(t & RMASK) * 16] = 0.0f;
+                  }
+                  range_err |= g > hi + RING_CELLS / 2;
+                  ring[(hi & RMASK) * 16] += extra;
+                  top = hi;
+               } else {
+                  // the slot holds nothing of this column's yet (its first
+                  // target's earlier content is already in acc)
+                  ring[soff] = acc;
+                  top = g;
+               }
+            }
+            // everything this block wrote must lie inside the ring's window
+            range_err |= top >= (next_flush + RING_BLOCKS) * WID;
+            // targets below the next source cell's lower bound are complete
+            int lb = ncf * WID;
+            if (kb < col_e) {
+               int nl = __reduce_min_sync(hmask, g < hi ? g : hi);
+               lb = (nl < lb) ? nl : lb;
+            }
+            flush_until(lb >> 2);
+            pw0 = cur[0]; pw1 = cur[1]; pw2 = cur[2]; pw3 = cur[3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+               cur[q] = nxt[q];
+               nxt[q] = nn[q];
+            }
+            ++src_rank;
+         }
+         col_s = nxt_s;
+         col_e = nxt_e;
+         cf = ncf;
+         cl = ncl;
+      }
+      flush_until(1 << 20);
+      if (__any_sync(hmask, range_err)) {
+         if (lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
+#pragma unroll
+         for (int q = 0; q < RING_CELLS; ++q) ring[q * 16] = 0.0f;
       }
    }
 }
@@ -741,25 +928,32 @@ cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
                          uint8_t* content_out, double content_threshold, bool exact, int recon, int grid,
                          cudaStream_t stream) {
-#define VLGPU_REMAP(D, E, R)                                                                                  \
-   remap_kernel<D, E, R><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids, \
-                                                             sweep_cells, status, mesh, wall_margin, set_capacity, \
-                                                             content_out, content_threshold)
-#define VLGPU_REMAP_DIMS(E, R)            \
-   if (dim == 0) VLGPU_REMAP(0, E, R);    \
-   else if (dim == 1) VLGPU_REMAP(1, E, R); \
-   else VLGPU_REMAP(2, E, R);
+#define VLGPU_REMAP(D)                                                                                        \
+   remap_kernel<D><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids,          \
+                                                       sweep_cells, status, mesh, wall_margin, set_capacity,        \
+                                                       content_out, content_threshold)
+#define VLGPU_WALK(D, R)                                                                                       \
+   remap_walk_kernel<D, R><<<grid, REMAP_THREADS, 0, stream>>>(sets, counters, perm, src_data, dst_data, dst_gids, \
+                                                               sweep_cells, status, mesh, wall_margin, set_capacity, \
+                                                               content_out, content_threshold)
+#define VLGPU_WALK_DIMS(R)               \
+   if (dim == 0) VLGPU_WALK(0, R);       \
+   else if (dim == 1) VLGPU_WALK(1, R);  \
+   else VLGPU_WALK(2, R);
    if (exact) {
       if (recon != RECON_PPM) return cudaErrorInvalidValue;  // the exact mode is PPM only
-      VLGPU_REMAP_DIMS(true, RECON_PPM)
+      if (dim == 0) VLGPU_REMAP(0);
+      else if (dim == 1) VLGPU_REMAP(1);
+      else VLGPU_REMAP(2);
    } else if (recon == RECON_PLM) {
-      VLGPU_REMAP_DIMS(false, RECON_PLM)
+      VLGPU_WALK_DIMS(RECON_PLM)
    } else if (recon == RECON_PQM) {
-      VLGPU_REMAP_DIMS(false, RECON_PQM)
+      VLGPU_WALK_DIMS(RECON_PQM)
    } else {
-      VLGPU_REMAP_DIMS(false, RECON_PPM)
+      VLGPU_WALK_DIMS(RECON_PPM)
    }
-#undef VLGPU_REMAP_DIMS
+#undef VLGPU_WALK_DIMS
+#undef VLGPU_WALK
 #undef VLGPU_REMAP
    return cudaGetLastError();
 }
@@ -775,7 +969,7 @@ cudaError_t launch_rebase_work(SweepCounters* counters, cudaStream_t stream) {
 
 int remap_blocks_per_sm() {
    int n = 0;
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_kernel<2, false, RECON_PPM>, REMAP_THREADS, 0);
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, remap_walk_kernel<2, RECON_PPM>, REMAP_THREADS, 0);
    return n > 0 ? n : 1;
 }
 

@@ -65,20 +65,6 @@ void free_batch(vlgpu_batch* b) {
    delete b;
 }
 
-// Per-cell sweep parameters in the swapped frame (cpu_acc_map.cpp:127-176).
-SweepCell make_sweep_cell(const double* I, uint32_t dim, double min_value) {
-   SweepCell s{};
-   float di = (float)I[1], dj = (float)I[2], dk = (float)I[3];
-   if (dim == 0) std::swap(di, dk);
-   if (dim == 1) std::swap(dj, dk);
-   s.intersection = (float)I[0];
-   s.di = di;
-   s.dj = dj;
-   s.dk = dk;
-   s.threshold = (float)min_value;
-   return s;
-}
-
 void set_direct_state(vlgpu_batch* b, int pool) {
    b->st_gids = b->gids[pool];
    b->st_src = nullptr;

@@ -5,38 +5,6 @@
 
 namespace vlgpu {
 
-// The same coefficients in plain single precision (fused mode): the superbee
-// slope as sign(a) * max(min(|a|, 2|b|), min(2|a|, |b|)) when a b > 0 (equal
-// to maxmod(minmod(a, 2b), minmod(2a, b)), whose minmod tests the same
-// product), on unscaled values, with contractible arithmetic.
-__device__ __forceinline__ void ppm_coeff_fused(float vm1, float v0, float vp1, float fl, float fr, float& a0,
-                                                float& a1, float& a2) {
-   const float a = vp1 - v0, b = v0 - vm1;
-   const bool same = a * b > 0.0f;
-   const float aa = fabsf(a), ab = fabsf(b);
-   const float sl = same ? fmaxf(fminf(aa, ab + ab), fminf(aa + aa, ab)) : 0.0f;
-   if (sl == 0.0f) {
-      fl = v0;
-      fr = v0;
-   }
-   const float hs = copysignf(0.5f * sl, a);
-   if ((vm1 - fl) * (fl - v0) < 0.0f) fl = v0 - hs;
-   if ((vp1 - fr) * (fr - v0) < 0.0f) fr = v0 + hs;
-   const float one_sixth = (float)(1.0 / 6.0);
-   const float v3 = 3.0f * v0;
-   {
-      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
-      if (d * e > d * d * one_sixth) fl = v3 - 2.0f * fr;
-   }
-   {
-      const float d = fr - fl, e = v0 - 0.5f * (fl + fr);
-      if (-d * d * one_sixth > d * e) fr = v3 - 2.0f * fl;
-   }
-   a0 = fl;
-   a1 = v3 - 2.0f * fl - fr;
-   a2 = fl + fr - 2.0f * v0;
-}
-
 // Superbee slope of (l, m, r) on unscaled values: sign(a) * max(min(|a|, 2|b|),
 // min(2|a|, |b|)) when a b > 0 (a = r - m, b = m - l), else 0.
 __device__ __forceinline__ float superbee_fused(float l, float m, float r) {
@@ -183,7 +151,10 @@ __device__ __forceinline__ float half_slope(float a, float b, float v0, float& f
    return copysignf(0.5f * sl, a);
 }
 
-// ppm_coeff_fused for two cells: f(t) = a0 + a1 t + a2 t^2 on each.
+// PPM coefficients of two cells at once (cpu_1d_ppm.hpp:35-54 in plain single
+// precision: superbee slope, faces outside their cells' values reset to
+// v0 -/+ slope/2, Colella-Woodward overshoot corrections): f(t) = a0 + a1 t +
+// a2 t^2 on each.
 __device__ __forceinline__ void ppm_coeff_x2(float2 vm1, float2 v0, float2 vp1, float2 fl, float2 fr, float2& a0,
                                              float2& a1, float2& a2) {
    const float2 a = p_sub(vp1, v0), b = p_sub(v0, vm1);

@@ -12,7 +12,8 @@
 // permutation, the column sets, the counters and the per-block content flags)
 // live here in one file-scope device array of fixed size, which every GPU
 // that loads libvlgpu.so keeps until the process exits.  The kernels are the
-// ones vlgpu_map_1d launches; only the place of their work arrays differs.
+// ones vlgpu_map_1d launches with its default (fused PPM) arithmetic; only the
+// place of their work arrays differs.
 #include <cstddef>
 #include <cstdio>
 #include <mutex>
@@ -57,12 +58,11 @@ struct NoallocLayout {
 
 // The scratch itself (about 3.3 MB).  In host code this name is only a
 // stand-in for the device variable: its device address comes from
-// cudaGetSymbolAddress, once per device.
+// cudaGetSymbolAddress, on every call.
 static __device__ __align__(256) unsigned char noalloc_scratch[sizeof(NoallocLayout)];
 
 struct DeviceSetup {
    bool ready;
-   unsigned char* base;  // device address of noalloc_scratch on this device
    int remap_grid;
 };
 std::mutex setup_mutex;
@@ -80,21 +80,23 @@ int na_status(cudaError_t e, const char* what) {
       if (_s != VLGPU_OK) return _s;        \
    } while (0)
 
-// First call on a device (that device current): the scratch's device address
-// and the remap grid size.
-int setup_device(int dev, DeviceSetup& out) {
+// Set-up of every call, with the calling device current: the device address
+// of noalloc_scratch (looked up each time, so that a context that was
+// destroyed and created again after an earlier call is served at the
+// scratch's new address) and, once per device, the remap grid size.
+int setup_device(int dev, unsigned char** base, int* remap_grid) {
+   void* ptr = nullptr;
+   NA_CHECK(cudaGetSymbolAddress(&ptr, noalloc_scratch));
+   *base = static_cast<unsigned char*>(ptr);
    std::lock_guard<std::mutex> lock(setup_mutex);
    DeviceSetup& s = setups[dev];
    if (!s.ready) {
-      void* ptr = nullptr;
-      NA_CHECK(cudaGetSymbolAddress(&ptr, noalloc_scratch));
       int sms = 0;
       NA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      s.base = static_cast<unsigned char*>(ptr);
       s.remap_grid = sms * remap_blocks_per_sm();
       s.ready = true;
    }
-   out = s;
+   *remap_grid = s.remap_grid;
    return VLGPU_OK;
 }
 
@@ -105,21 +107,6 @@ __global__ void check_gids_kernel(const uint32_t* __restrict__ gids, uint64_t be
    for (uint64_t q = begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < end;
         q += (uint64_t)gridDim.x * blockDim.x)
       if (gids[q] >= max_gid) atomicOr(bad, 1u);
-}
-
-// Per-cell sweep parameters in the swapped frame (cpu_acc_map.cpp:127-176);
-// the same conversion vlgpu_map_1d applies.
-SweepCell sweep_cell(const double* I, uint32_t dim, double min_value) {
-   SweepCell s{};
-   float di = (float)I[1], dj = (float)I[2], dk = (float)I[3];
-   if (dim == 0) { const float t = di; di = dk; dk = t; }
-   if (dim == 1) { const float t = dj; dj = dk; dk = t; }
-   s.intersection = (float)I[0];
-   s.di = di;
-   s.dj = dj;
-   s.dk = dk;
-   s.threshold = (float)min_value;
-   return s;
 }
 
 }  // namespace
@@ -154,6 +141,10 @@ extern "C" int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* 
    }
    if (end > begin && (!gids_in || !data_in)) return VLGPU_EINVAL;
    if (out_capacity > 0 && (!gids_out || !data_out)) return VLGPU_EINVAL;
+   if (end > begin && ((const void*)data_out == (const void*)data_in || (const void*)gids_out == (const void*)gids_in)) {
+      std::fprintf(stderr, "vlgpu_map_1d_noalloc: the output buffers must not be the input buffers\n");
+      return VLGPU_EINVAL;
+   }
    if ((reinterpret_cast<uintptr_t>(data_in) | reinterpret_cast<uintptr_t>(data_out)) & 15u) {
       std::fprintf(stderr, "vlgpu_map_1d_noalloc: data_in and data_out must be 16-byte aligned\n");
       return VLGPU_EINVAL;
@@ -162,13 +153,13 @@ extern "C" int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* 
    int dev = 0;
    NA_CHECK(cudaGetDevice(&dev));
    if (dev < 0 || dev >= NA_MAX_DEVICES) return VLGPU_ENODEV;
-   DeviceSetup setup{};
-   const int st = setup_device(dev, setup);
+   unsigned char* base = nullptr;  // device address of noalloc_scratch on this device
+   int remap_grid = 0;
+   const int st = setup_device(dev, &base, &remap_grid);
    if (st != VLGPU_OK) return st;
    cudaStream_t s = static_cast<cudaStream_t>(stream);
 
    // device views of the scratch
-   unsigned char* base = setup.base;
    SweepCounters* d_counters = reinterpret_cast<SweepCounters*>(base + offsetof(NoallocLayout, counters));
    uint32_t* d_bad = reinterpret_cast<uint32_t*>(base + offsetof(NoallocLayout, bad_gid));
    BatchStats* d_stats = reinterpret_cast<BatchStats*>(base + offsetof(NoallocLayout, stats));
@@ -185,7 +176,7 @@ extern "C" int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* 
    CellSlot h_slots[NA_MAX_CELLS];
    uint32_t h_status[NA_MAX_CELLS];
    for (uint32_t c = 0; c < n_cells; ++c) {
-      h_sweep[c] = sweep_cell(intersections + 4 * (size_t)c, dimension, params->min_value);
+      h_sweep[c] = make_sweep_cell(intersections + 4 * (size_t)c, dimension, params->min_value);
       h_slots[c].off = (uint32_t)offsets[c];
       h_slots[c].count = (uint32_t)(offsets[c + 1] - offsets[c]);
    }
@@ -222,7 +213,7 @@ extern "C" int vlgpu_map_1d_noalloc(const vlgpu_mesh* mesh, const vlgpu_params* 
                              NA_MAX_BLOCKS, dst_cap, d_sweep, d_status, d_counters, d_stats, mdev, wm, 0, n_cells, 0,
                              s));
    NA_CHECK(launch_remap((int)dimension, d_sets, d_counters, d_perm, data_in, data_out, gids_out, d_sweep, d_status,
-                         mdev, wm, NA_MAX_BLOCKS, d_content, params->min_value, false, 2, setup.remap_grid, s));
+                         mdev, wm, NA_MAX_BLOCKS, d_content, params->min_value, false, 2, remap_grid, s));
 
    SweepCounters h_counters{};
    NA_CHECK(cudaMemcpyAsync(h_slots, d_dst_slots, sizeof(CellSlot) * n_cells, cudaMemcpyDeviceToHost, s));

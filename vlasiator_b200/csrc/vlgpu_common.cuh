@@ -39,6 +39,24 @@ struct SweepCell {
    uint32_t pad;
 };
 
+// Per-cell sweep parameters of one dimension from the four doubles
+// (intersection, di, dj, dk) the reference stores per population, cast to
+// Realf and swapped into the frame where the sweep dimension is k
+// (cpu_acc_map.cpp:127-176).  Every entry point that sweeps uses this one
+// conversion.
+inline SweepCell make_sweep_cell(const double* I, uint32_t dim, double min_value) {
+   SweepCell s{};
+   float di = (float)I[1], dj = (float)I[2], dk = (float)I[3];
+   if (dim == 0) { const float t = di; di = dk; dk = t; }
+   if (dim == 1) { const float t = dj; dj = dk; dk = t; }
+   s.intersection = (float)I[0];
+   s.di = di;
+   s.dj = dj;
+   s.dk = dk;
+   s.threshold = (float)min_value;
+   return s;
+}
+
 // Mesh constants used on the device (cell size and origin already in Realf),
 // with the reciprocals of block_xyz (zero: plain division).
 struct MeshDev {
