@@ -130,9 +130,10 @@ int vlgpu_map_1d_per_cell(vlgpu_batch* b, const double* intersections, uint32_t 
    batch would use.  It has no counterpart in the reference: it exists for
    host codes that reserve all of the GPU's memory for their own pool at
    start-up, and for codes that call the sweep on a latency-critical path,
-   where a cudaMalloc/cudaFree would synchronise the whole device.  It allocates nothing: its work arrays live
-   in one fixed device array of about 3.3 MB inside libvlgpu.so, held by every
-   GPU that loads the library until the process exits.
+   where a cudaMalloc/cudaFree would synchronise the whole device.  It
+   allocates nothing: its work arrays live in one fixed device array of about
+   3.3 MB inside libvlgpu.so, held by every GPU that loads the library until
+   the process exits.
    Limits per call: 1..VLGPU_NOALLOC_MAX_CELLS cells, input block indices
    below VLGPU_NOALLOC_MAX_BLOCKS (offsets[n_cells] <= the limit) and at most
    VLGPU_NOALLOC_MAX_BLOCKS output blocks; larger inputs are rejected with
@@ -177,7 +178,12 @@ int vlgpu_accelerate_with_intersections(vlgpu_batch* b, const double* intersecti
    blocks are adjusted (adjustVelocityBlocks, grid.cpp:775-817, cells without
    spatial neighbours) and the moments including the pressure tensor are
    recomputed.  fields: one vlgpu_cell_fields per cell; dt: one substep length
-   per cell (Population::subcycleDt); host memory. */
+   per cell (Population::subcycleDt); host memory.  A cell whose dt is 0 is
+   not accelerated: its blocks pass through the sweeps unchanged, as the
+   reference leaves cells that have finished their subcycles out of the
+   accelerated cells (vlasovmover.cpp:547-556) and does no remap when dt is 0
+   (vlasovmover.cpp:490-497); its block adjustment and moments still run, and
+   adjusting an already adjusted cell changes nothing. */
 int vlgpu_accelerate(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt, uint32_t map_order);
 
 /* Only the geometry part of that step: pivot moments, FP64 transform and the

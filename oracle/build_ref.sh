@@ -54,6 +54,12 @@ sed -n '1,443p' "$REF/vlasovsolver/cpu_trans_map_amr.cpp" > "$SRC/vlasovsolver/c
   printf '}  // namespace spatial_cell\n'
   sed -n '28,119p' "$REF/spatial_cells/block_adjust_cpu.cpp"
 } > "$SRC/spatial_cells/block_adjust_part.cpp"
+# the r-space time-step reduction reduce_vlasov_dt (arch_dt.cpp, the whole
+# file); its source names std types unqualified
+{
+  printf '#include <algorithm>\n#include <limits>\n#include <vector>\nusing namespace std;\n'
+  cat "$REF/vlasovsolver/arch_dt.cpp"
+} > "$SRC/vlasovsolver/arch_dt_part.cpp"
 cp "$HERE/ref_shim/grid.h" "$SRC/grid.h"
 cp "$HERE/ref_shim/object_wrapper.h" "$SRC/object_wrapper.h"
 cp "$HERE/ref_shim/spatial_cells/spatial_cell_wrapper.hpp" "$SRC/spatial_cells/spatial_cell_wrapper.hpp"
@@ -67,7 +73,7 @@ COMMON=(-std=c++20 -O3 -march=x86-64-v3 -ffp-contract=off -fopenmp -fPIC -shared
 SRCS=("$SRC/ref_harness.cpp" "$SRC/vlasovsolver/cpu_acc_map.cpp"
       "$SRC/vlasovsolver/cpu_acc_sort_blocks.cpp" "$SRC/vlasovsolver/cpu_acc_load_blocks.cpp"
       "$SRC/velocity_mesh_parameters.cpp" "$SRC/vlasovsolver/cpu_trans_map_amr_part.cpp"
-      "$SRC/spatial_cells/block_adjust_part.cpp")
+      "$SRC/spatial_cells/block_adjust_part.cpp" "$SRC/vlasovsolver/arch_dt_part.cpp")
 # the oracle's own FP64 geometry restatement (the reference's needs Eigen)
 CC="${REF_CC:-/usr/bin/gcc}"
 "$CC" -O2 -std=c11 -fPIC -ffp-contract=off -c "$HERE/vlasov_oracle.c" -o "$OUT/orc_geometry_sp.o"

@@ -271,6 +271,8 @@ class ReferenceBuild:
         L.ref_cells_create.restype = _vp
         L.ref_cells_create.argtypes = [ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64), _u32p, ctypes.POINTER(ct), _dp]
         L.ref_cells_destroy.argtypes = [_vp]
+        L.ref_cells_count.restype = ctypes.c_uint32
+        L.ref_cells_count.argtypes = [_vp]
         L.ref_cells_block_count.restype = ctypes.c_uint64
         L.ref_cells_block_count.argtypes = [_vp, ctypes.c_uint32]
         L.ref_cells_extract.restype = ctypes.c_uint64
@@ -286,6 +288,10 @@ class ReferenceBuild:
                                           ctypes.c_int]
         L.ref_cells_adjust.argtypes = [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_cells_max_r_dt.restype = ctypes.c_double
+        L.ref_cells_max_r_dt.argtypes = [_vp, _dp, _dp]
+        L.ref_map_order.restype = ctypes.c_uint32
+        L.ref_map_order.argtypes = [ctypes.c_uint32]
         L.ref_cells_content.restype = ctypes.c_uint64
         L.ref_cells_content.argtypes = [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64]
 
@@ -362,6 +368,19 @@ class ReferenceBuild:
         self.lib.ref_cells_adjust(h, nb, k, float(min_value), int(add_width), int(conserve_mass), nthreads,
                                   _ptr(loss, ctypes.c_double))
         return loss
+
+    def max_r_dt(self, h, dx):
+        """reduce_vlasov_dt (arch_dt.cpp:33-97) over the set: each cell's MAXRDT
+        and the minimum over the cells."""
+        n = self.lib.ref_cells_count(h)
+        out = np.zeros(n)
+        d = np.ascontiguousarray(dx, np.float64)
+        total = self.lib.ref_cells_max_r_dt(h, _ptr(d, ctypes.c_double), _ptr(out, ctypes.c_double))
+        return out, total
+
+    def map_order(self, tstep: int) -> int:
+        """The dimension order the reference draws for time step tstep (vlasovmover.cpp:422-426)."""
+        return int(self.lib.ref_map_order(int(tstep)))
 
     def content(self, h, c):
         """compute_block_has_content of cell c's blocks, in local-ID order."""

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 #include <omp.h>
+#include <random>
 
 #include "memoryallocation.h"
 #include "object_wrapper.h"
@@ -28,6 +29,9 @@ void update_velocity_block_content_lists(dccrg::Dccrg<SpatialCell, dccrg::Cartes
 void adjust_velocity_blocks_in_cells(dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry>& mpiGrid,
                                      const std::vector<CellID>& cellsToAdjust, const uint popID);
 }  // namespace spatial_cell
+// the reference's r-space time-step reduction (vlasovsolver/arch_dt.cpp:33-97)
+void reduce_vlasov_dt(dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry>& mpiGrid, const std::vector<CellID>& cells,
+                      Real (&dtMaxLocal)[3]);
 
 using spatial_cell::SpatialCell;
 
@@ -37,6 +41,7 @@ Real Parameters::hallMinimumRhoq = 1.60217653e-19;
 uint Parameters::ohmGradPeTerm = 0;
 bool Parameters::prepareForRebalance = false;
 uint Parameters::tstep = 0;
+bool Parameters::vlasovAccelerateMaxwellianBoundaries = false;
 
 static ObjectWrapper g_objects;
 ObjectWrapper& getObjectWrapper() { return g_objects; }
@@ -116,6 +121,8 @@ void ref_cells_destroy(void* h) {
    for (auto* c : rc->cells) delete c;
    delete rc;
 }
+
+uint32_t ref_cells_count(void* h) { return (uint32_t)((RefCells*)h)->cells.size(); }
 
 uint64_t ref_cells_block_count(void* h, uint32_t c) { return ((RefCells*)h)->cells[c]->get_velocity_mesh(0)->size(); }
 
@@ -274,6 +281,41 @@ uint64_t ref_cells_content(void* h, uint32_t c, uint8_t* flags, uint64_t cap) {
    if (n > cap) return n;
    for (uint64_t lid = 0; lid < n; ++lid) flags[lid] = sc->compute_block_has_content((vmesh::LocalID)lid, 0) ? 1 : 0;
    return n;
+}
+
+// The r-space time-step limit of every cell of the set with the reference's
+// own reduce_vlasov_dt (vlasovsolver/arch_dt.cpp:33-97): the minimum over the
+// cell's blocks of dx/|v| at the centres of the block's first and last
+// cells.  dx: the cell sizes (DX, DY, DZ); r_dt gets each cell's MAXRDT;
+// returns the reduction over all cells (dtMaxLocal[0]).
+double ref_cells_max_r_dt(void* h, const double dx[3], double* r_dt) {
+   RefCells* rc = (RefCells*)h;
+   dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry> g;
+   std::vector<CellID> cells;
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      SpatialCell* sc = rc->cells[c];
+      sc->parameters[CellParams::DX] = dx[0];
+      sc->parameters[CellParams::DY] = dx[1];
+      sc->parameters[CellParams::DZ] = dx[2];
+      sc->parameters[CellParams::MAXVDT] = 0;
+      g.cells[c + 1] = sc;
+      cells.push_back(c + 1);
+   }
+   Real dt_max[3] = {std::numeric_limits<Real>::max(), std::numeric_limits<Real>::max(),
+                     std::numeric_limits<Real>::max()};
+   reduce_vlasov_dt(g, cells, dt_max);
+   for (size_t c = 0; c < rc->cells.size(); ++c) r_dt[c] = rc->cells[c]->parameters[CellParams::MAXRDT];
+   return dt_max[0];
+}
+
+// The dimension order of time step `tstep`, drawn as calculateAcceleration
+// draws it for every subcycle of that step (vlasovsolver/vlasovmover.cpp:
+// 422-426): a default_random_engine seeded with the step number and one
+// uniform_int_distribution<>(0, 2) draw, with this compiler's standard library.
+uint32_t ref_map_order(uint32_t tstep) {
+   std::default_random_engine rndState;
+   rndState.seed(tstep);
+   return (uint32_t)std::uniform_int_distribution<>(0, 2)(rndState);
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }

@@ -37,5 +37,6 @@ struct Parameters {
    static uint ohmGradPeTerm;
    static bool prepareForRebalance;
    static uint tstep;
+   static bool vlasovAccelerateMaxwellianBoundaries;
 };
 typedef Parameters P;

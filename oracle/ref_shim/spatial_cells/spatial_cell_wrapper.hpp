@@ -8,7 +8,8 @@
 // helpers below follow their counterparts in spatial_cells/spatial_cell_cpu.hpp:
 // add_velocity_block (:757-768) and remove_velocity_block (:826-850, "move the
 // last block into the hole"), get_velocity_block_indices / get_velocity_block
-// (:535-550), get_block_parameters (:445-462).  The block-adjustment member
+// (:535-550), get_block_parameters (:445-462), get/set_max_r_dt
+// (spatial_cell_cpu.cpp:322-352).  The block-adjustment member
 // functions themselves (adjust_velocity_blocks, compute_block_has_content,
 // update_velocity_block_content_lists, updateSparseMinValue) are the
 // reference's own definitions, compiled from spatial_cell_cpu.cpp.
@@ -34,6 +35,7 @@ struct Population {
    Real velocityBlockMinValue{0};
    Real RHOLOSSADJUST{0};
    Real RHO{0};
+   Real max_dt[2]{0, 0};  // species::MAXRDT, species::MAXVDT
    Population() {
       vmesh = new vmesh::VelocityMesh();
       blockContainer = new vmesh::VelocityBlockContainer();
@@ -52,6 +54,8 @@ class SpatialCell {
    std::deque<Population> populations;
    std::vector<vmesh::GlobalID>* velocity_block_with_content_list;
    std::vector<vmesh::GlobalID>* velocity_block_with_no_content_list;
+   uint sysBoundaryFlag{sysboundarytype::NOT_SYSBOUNDARY};
+   uint sysBoundaryLayer{0};
 
    explicit SpatialCell(size_t nPops = 1) {
       for (auto& p : parameters) p = 0;
@@ -73,6 +77,8 @@ class SpatialCell {
    static vmesh::GlobalID invalid_global_id() { return vmesh::INVALID_GLOBALID; }
    static vmesh::LocalID invalid_local_id() { return vmesh::INVALID_LOCALID; }
    void debug_population_check(const uint) const {}
+   void set_max_r_dt(const uint popID, const Real& value) { populations[popID].max_dt[0] = value; }
+   const Real& get_max_r_dt(const uint popID) const { return populations[popID].max_dt[0]; }
    vmesh::LocalID get_number_of_velocity_blocks(const uint popID) const { return populations[popID].vmesh->size(); }
    vmesh::LocalID get_velocity_block_local_id(const vmesh::GlobalID& gid, const uint popID) const {
       return populations[popID].vmesh->getLocalID(gid);

@@ -13,8 +13,10 @@ mode, values agree to 1e-5 of the cell's peak and block sets to 1%.
 import numpy as np
 import pytest
 
+from oracle.oracle import ReferenceBuild, reference_available
 from vlasiator_b200.grid import grid_neighbors
 from vlasiator_b200.mesh import CHARGE, MASS_PROTON, WID3
+from tests.grid_cases import r_dt_restated, varied_grid
 from vlasiator_b200.projects import maxwellian_cell, sinewave_grid
 
 pytestmark = pytest.mark.gpu
@@ -27,33 +29,6 @@ def vl():
     from vlasiator_b200 import vlgpu
     vlgpu.load()
     return vlgpu
-
-
-def varied_grid(mesh, dims, seed):
-    rng = np.random.default_rng(seed)
-    cells = []
-    for _ in range(int(np.prod(dims))):
-        V = rng.uniform(-3e5, 3e5, 3)
-        cells.append(maxwellian_cell(mesh, 10 ** rng.uniform(5.5, 6.5), rng.uniform(1.5e5, 4e5), V))
-    return cells
-
-
-def r_dt_restated(mesh, cells, dx):
-    """reduce_vlasov_dt for one population, in numpy (arch_dt.cpp:34-97)."""
-    eps = np.finfo(np.float64).tiny * 1000
-    bs = [(mesh.vmax[d] - mesh.vmin[d]) / mesh.length[d] for d in range(3)]
-    dv = [bs[d] / 4 for d in range(3)]
-    out = []
-    for c in cells:
-        g = c.gids.astype(np.int64)
-        idx = [g % mesh.length[0], (g // mesh.length[0]) % mesh.length[1], g // (mesh.length[0] * mesh.length[1])]
-        best = np.inf
-        for i in (0, 3):
-            V = [mesh.vmin[d] + idx[d] * bs[d] + (i + 0.5) * dv[d] + eps for d in range(3)]
-            t = np.minimum(np.minimum(dx[0] / np.abs(V[0]), dx[1] / np.abs(V[1])), dx[2] / np.abs(V[2]))
-            best = min(best, float(t.min()))
-        out.append(best)
-    return np.array(out)
 
 
 def test_spatial_adjust_matches_oracle(vl, mesh, orc_sp):
@@ -95,6 +70,17 @@ def test_max_dt_matches_restatement(vl, mesh):
         b.compute_intersections(B, 0.01, 0)  # stages the fields
         r, v = b.max_dt(22.0)
     np.testing.assert_array_equal(r, r_dt_restated(mesh, cells, dx))
+    if reference_available("sp"):
+        # and the reference's own reduce_vlasov_dt (arch_dt.cpp:33-97)
+        ref = ReferenceBuild("sp")
+        ref.init(mesh)
+        h = ref.create([c.gids for c in cells], [c.data for c in cells], [1e-15] * len(cells))
+        try:
+            r_ref, total = ref.max_r_dt(h, dx)
+        finally:
+            ref.destroy(h)
+        np.testing.assert_array_equal(r, r_ref)
+        assert total == r.min()
     Bm = np.sqrt((B ** 2).sum(1)) + 1e-30
     np.testing.assert_allclose(v, np.abs(2 * np.pi * MASS_PROTON / (CHARGE * Bm)) * (22.0 / 360.0), rtol=1e-15)
 

@@ -50,3 +50,31 @@ def test_subcycle_sequence():
     np.testing.assert_allclose(steps[:, 0], [0.4, 0.4, 0.1, 0.0])
     np.testing.assert_allclose(steps[:, 1], [0.9, 0.0, 0.0, 0.0])
     assert (subcycle_dt(0, -dt, mvdt) <= 0).all()
+
+
+def test_subcycle_counts_follow_the_reference_formula():
+    # getAccelerationSubcycles takes ceil(dt / max_v_dt) of the signed dt
+    # (vlasovmover.cpp:398-401): a negative dt gives one subcycle
+    from vlasiator_b200.populations import cell_subcycles
+    m = np.array([0.4, 1.0, 0.25])
+    np.testing.assert_array_equal(cell_subcycles(0.9, m), [3, 1, 4])
+    np.testing.assert_array_equal(cell_subcycles(0.8, m), [2, 1, 4])
+    np.testing.assert_array_equal(cell_subcycles(-0.9, m), [1, 1, 1])
+
+
+def test_map_order_matches_the_reference_draw():
+    """map_order_for_step against the reference's own draw
+    (vlasovmover.cpp:422-426) compiled with this machine's C++ library."""
+    import pytest
+
+    from oracle.oracle import ReferenceBuild, reference_available
+    from vlasiator_b200.populations import map_order_for_step
+    if not reference_available("sp"):
+        pytest.skip("reference build (oracle/_ref) not present")
+    ref = ReferenceBuild("sp")
+    # the first draw is 16807 t: every step below about 42,590 gets order 0
+    steps = list(range(0, 200)) + list(range(40000, 2000000, 7919)) + [2 ** 31 - 2, 2 ** 31 - 1, 123456789]
+    got = [map_order_for_step(t) for t in steps]
+    assert got == [ref.map_order(t) for t in steps]
+    assert set(got) == {0, 1, 2}
+    assert set(got[:200]) == {0}

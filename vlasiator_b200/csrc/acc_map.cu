@@ -279,16 +279,22 @@ __global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
       const uint32_t si = a_lo + t / nb, sj = b_lo + t % nb;
       uint32_t m[3] = {mask[3 * t], mask[3 * t + 1], mask[3 * t + 2]};
       uint32_t tm[3] = {0u, 0u, 0u};
-      float mx, mn;
-      set_corners(P, si, sj, mx, mn);
-      if (!(P.dk > 0.0f)) baddk = 1;
-      int k = mask_next_set(m, 0);
-      while (k < 96) {
-         const int e = mask_next_clear(m, k) - 1;
-         int fb, lb;
-         if (column_extent(mx, mn, P.dk, mesh.dv[DIM], mesh.vmin[DIM], max_len, k, e, wall_margin, fb, lb)) wall = 1;
-         for (int q = fb; q <= lb; ++q) tm[q >> 5] |= 1u << (q & 31);
-         k = mask_next_set(m, e + 1);
+      if (P.flags & SWEEP_PASS) {
+         // the cell's blocks pass through the sweep unchanged
+         tm[0] = m[0]; tm[1] = m[1]; tm[2] = m[2];
+      } else {
+         float mx, mn;
+         set_corners(P, si, sj, mx, mn);
+         if (!(P.dk > 0.0f)) baddk = 1;
+         int k = mask_next_set(m, 0);
+         while (k < 96) {
+            const int e = mask_next_clear(m, k) - 1;
+            int fb, lb;
+            if (column_extent(mx, mn, P.dk, mesh.dv[DIM], mesh.vmin[DIM], max_len, k, e, wall_margin, fb, lb))
+               wall = 1;
+            for (int q = fb; q <= lb; ++q) tm[q >> 5] |= 1u << (q & 31);
+            k = mask_next_set(m, e + 1);
+         }
       }
       tcount[s] = __popc(tm[0]) + __popc(tm[1]) + __popc(tm[2]);
       if (sets_ok) {
@@ -407,6 +413,31 @@ __device__ __forceinline__ void store_lane(float* __restrict__ blk, int i, int j
    }
 }
 
+// The set of a cell that is not accelerated in this step (SWEEP_PASS): its
+// blocks are copied to the output in ascending k, which is the target mask's
+// order (columnize gave the set its source mask as the target mask), with
+// their block IDs and content flags.
+template <int DIM>
+__device__ __forceinline__ void pass_through_set(const ColumnSet& cs, const uint32_t* __restrict__ perm,
+                                                 const float* __restrict__ src_data, float* __restrict__ dst_data,
+                                                 uint32_t* __restrict__ dst_gids, uint8_t* __restrict__ content_out,
+                                                 const MeshDev& mesh, float content_thr, int lane, unsigned hmask) {
+   const int i = lane & 3, j = lane >> 2;
+   uint32_t r = 0;
+   for (int k = mask_next_set(cs.src_mask, 0); k < 96; k = mask_next_set(cs.src_mask, k + 1), ++r) {
+      float v[4];
+      load_lane<DIM>(src_data, perm[cs.src_pos + r], i, j, v);
+      const uint32_t o = cs.dst_pos + r;
+      store_lane<DIM>(dst_data + (size_t)o * WID3, i, j, v);
+      const bool c = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3])) >= content_thr;
+      const unsigned any_c = __ballot_sync(hmask, c) & hmask;
+      if (lane == 0) {
+         dst_gids[o] = gid_from_swapped(cs.si, cs.sj, (uint32_t)k, mesh.len, DIM);
+         content_out[o] = any_c ? 1 : 0;
+      }
+   }
+}
+
 // Reference argmax / argmin lane selection (cpu_acc_map.cpp:515-529): the
 // first lane holding the largest value above DBL_MIN (default lane 0) and the
 // first lane holding the smallest value below DBL_MAX (default lane 0).
@@ -463,6 +494,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
       if (sidx >= n_sets) break;
       const ColumnSet cs = sets[sidx];
       const SweepCell P = sweep_cells[cs.cell];
+      if (P.flags & SWEEP_PASS) {
+         pass_through_set<DIM>(cs, perm, src_data, dst_data, dst_gids, content_out, mesh, content_thr, lane, hmask);
+         continue;
+      }
       const float threshold = P.threshold;
       const float scale = __double2float_rn(1.0 / (double)threshold);
       const float dk = P.dk;
@@ -671,6 +706,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) rem
       if (sidx >= n_sets) break;
       const ColumnSet cs = sets[sidx];
       const SweepCell P = sweep_cells[cs.cell];
+      if (P.flags & SWEEP_PASS) {
+         pass_through_set<DIM>(cs, perm, src_data, dst_data, dst_gids, content_out, mesh, content_thr, lane, hmask);
+         continue;
+      }
       const float dk = P.dk;
       const float A = fa((float)(cs.si * WID), (float)i);
       const float B = fa((float)(cs.sj * WID), (float)j);

@@ -355,7 +355,7 @@ __global__ void geometry_kernel(const CellAccelInputs* __restrict__ in, const do
       s.dj = dj;
       s.dk = dk;
       s.threshold = threshold;
-      s.pad = 0;
+      s.flags = (a.dt == 0.0) ? SWEEP_PASS : 0u;
       sweep3[(size_t)d * n_cells + c] = s;
    }
 }

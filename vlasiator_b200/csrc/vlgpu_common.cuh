@@ -36,8 +36,13 @@ struct ColumnSet {
 struct SweepCell {
    float intersection, di, dj, dk;
    float threshold;
-   uint32_t pad;
+   uint32_t flags;  // SWEEP_PASS
 };
+
+// The cell is not accelerated in this step (its substep length is zero, as
+// for a cell that has finished its subcycles, vlasovmover.cpp:527-556): the
+// sweep passes its blocks through unchanged.
+constexpr uint32_t SWEEP_PASS = 1u;
 
 // Per-cell sweep parameters of one dimension from the four doubles
 // (intersection, di, dj, dk) the reference stores per population, cast to

@@ -44,28 +44,64 @@ def combine_moments(records, masses, charges) -> np.ndarray:
     return out
 
 
+def cell_subcycles(dt: float, max_v_dt) -> np.ndarray:
+    """Subcycles per cell, getAccelerationSubcycles (vlasovmover.cpp:398-401):
+    max(ceil(dt / max_v_dt), 1), with dt signed as the reference passes it."""
+    m = np.atleast_1d(np.asarray(max_v_dt, np.float64))
+    return np.maximum(np.ceil(dt / m), 1).astype(np.int64)
+
+
 def acceleration_subcycles(dt: float, max_v_dt) -> int:
-    """Global subcycle count (getAccelerationSubcycles, vlasovmover.cpp:398-401,
-    maxed over cells as vlasovmover.cpp:527-545 does)."""
-    return max(1, max(int(math.ceil(abs(dt) / float(m))) for m in np.atleast_1d(max_v_dt)))
+    """Global subcycle count: the maximum over cells (vlasovmover.cpp:527-545)."""
+    return int(cell_subcycles(dt, max_v_dt).max())
 
 
 def subcycle_dt(step: int, dt: float, max_v_dt) -> np.ndarray:
     """Per-cell dt of subcycle `step` (calculateAcceleration, vlasovmover.cpp:
-    428-456): max_v_dt on every step but the last, which takes the rest;
-    zero once a cell has covered |dt|; the sign of dt."""
-    m = np.asarray(max_v_dt, np.float64)
+    428-456): max_v_dt on every step but the last, which takes the rest, with
+    the sign of dt; zero for a cell whose subcycles are done (the reference
+    leaves it out of the accelerated cells, vlasovmover.cpp:547-556)."""
+    m = np.atleast_1d(np.asarray(max_v_dt, np.float64))
     this = np.where((step + 1) * m > abs(dt), np.maximum(abs(dt) - step * m, 0.0), m)
+    this = np.where(step < cell_subcycles(dt, m), this, 0.0)
     return -this if dt < 0 else this
 
 
-def accelerate_subcycled(batch, B, dt: float, max_v_dt, map_orders) -> int:
-    """Acceleration over dt in subcycles of at most max_v_dt per cell, each a
+# std::minstd_rand0 (std::default_random_engine of the GNU C++ library):
+# x <- 16807 x mod (2^31 - 1), seeded with s mod (2^31 - 1) (1 for 0)
+_MINSTD_A, _MINSTD_M = 16807, 2147483647
+
+
+def map_order_for_step(tstep: int) -> int:
+    """The dimension order of every subcycle of time step `tstep`
+    (calculateAcceleration, vlasovmover.cpp:422-426): one draw of
+    uniform_int_distribution<>(0, 2) from a default_random_engine seeded with
+    the step number.  The GNU C++ library's distribution scales down the
+    engine's range [1, 2^31 - 2] by (range // 3), rejecting draws past 3 times
+    that."""
+    x = tstep % _MINSTD_M
+    if x == 0:
+        x = 1
+    urange = _MINSTD_M - 2 - 1          # engine max - min
+    scaling = urange // 3
+    past = 3 * scaling
+    while True:
+        x = (_MINSTD_A * x) % _MINSTD_M
+        r = x - 1
+        if r < past:
+            return r // scaling
+
+
+def accelerate_subcycled(batch, B, dt: float, max_v_dt, map_order: int) -> int:
+    """Acceleration of one population over dt in subcycles of at most max_v_dt
+    per cell, as calculateAcceleration does it (vlasovmover.cpp:503-565): all
+    subcycles of the step in one dimension order (map_order_for_step), each a
     full vlgpu_accelerate step (pivot moments, three sweeps, block adjustment,
-    moments).  Cells that have covered dt before the last subcycle take dt = 0
-    steps, where the reference leaves them out of the accelerated cells.
-    Returns the number of subcycles."""
+    moments).  A cell whose subcycles are done gets dt = 0 and passes through
+    unchanged; the adjustment that follows the last subcycle is the
+    reference's final adjustVelocityBlocks of all cells, and adjusting an
+    already adjusted cell changes nothing.  Returns the number of subcycles."""
     n = acceleration_subcycles(dt, max_v_dt)
     for s in range(n):
-        batch.accelerate(B, subcycle_dt(s, dt, max_v_dt), map_orders[s % len(map_orders)])
+        batch.accelerate(B, subcycle_dt(s, dt, max_v_dt), map_order)
     return n
