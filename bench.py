@@ -52,6 +52,7 @@ BYTES_PER_CELL_SWEEP = 8  # read + write one fp32 phase-space cell per 1D sweep
 # 512-cell case of this workload (705,499 blocks), fused arithmetic; scaled by
 # the source blocks of a launch to give the full-size traffic per launch.
 REMAP_DRAM_BYTES_PER_BLOCK = 380.0e6 / 705499
+DEFAULT_SEED = 2026  # the workload's seed unless --seed says otherwise
 
 
 def workload(n_cells: int, seed: int):
@@ -163,61 +164,74 @@ def allreduce_sum(pg, x: float) -> float:
 # CPU baseline: the reference's own map_1d (oracle/_ref) on host cores
 # ---------------------------------------------------------------------------
 def cpu_reference_rate(mesh, offs, gids, data, B, dt, orders, sample_cells, target_s=12.0):
-    """Times the reference's acceleration step on a bounded sample of cells with
-    all host threads; returns (cell-updates/s, cores, sample description)."""
-    from oracle.oracle import ReferenceBuild, Restatement, reference_available  # CPU baseline leg only
+    """Times the reference's full acceleration step (pivot moments, geometry,
+    map_1d x3, adjustVelocityBlocks, moments with pressure) on the workload's
+    cells with all host threads, as many steps as fit in about target_s;
+    returns (cell-updates/s, cores, sample description, kind) or None."""
+    from oracle.oracle import ReferenceBuild, reference_available  # CPU baseline leg only
+    if not reference_available("sp"):
+        return None
     n = min(sample_cells, len(offs) - 1)
     glist = [gids[offs[c]:offs[c + 1]] for c in range(n)]
     dlist = [data[offs[c]:offs[c + 1]] for c in range(n)]
-    if reference_available("sp"):
-        ref = ReferenceBuild("sp")
-        kind = "reference"
-    else:
-        return None
+    ref = ReferenceBuild("sp")
     ref.init(mesh)
     cores = ref.max_threads()
-    updates = 0
-    elapsed = 0.0
-    reps = 0
+    h = ref.create(glist, dlist, [1e-15] * n)
+    updates, elapsed, reps = 0, 0.0, 0
     while elapsed < target_s and reps < 64:
-        h = ref.create(glist, dlist, [1e-15] * n)
         blocks = sum(ref.lib.ref_cells_block_count(h, c) for c in range(n))
         t0 = time.perf_counter()
-        ref.accelerate_step(h, B[:n], dt[:n], orders[reps % len(orders)], CHARGE, MASS_PROTON, 0)
+        ref.full_step(h, B[:n], dt[:n], orders[reps % len(orders)], CHARGE, MASS_PROTON)
         elapsed += time.perf_counter() - t0
         updates += WID3 * blocks
-        ref.destroy(h)
         reps += 1
-    _ = Restatement  # the restatement is not timed
-    return updates / elapsed, cores, f"{n} of the workload's cells x {reps} steps ({updates} cell-updates)", kind
+    ref.destroy(h)
+    what = "all" if n == len(offs) - 1 else f"the first {n} of the"
+    return (updates / elapsed, cores,
+            f"{what} {len(offs) - 1} cells of the workload x {reps} full acceleration steps ({updates} "
+            f"cell-updates): the reference's map_1d, adjust_velocity_blocks and moment templates", "reference")
 
 
 def cpu_vlasov_rate(dims, target_s=12.0):
-    """Times the oracle's full Vlasov step (the C restatement driven per cell,
-    one host thread) on a small grid of the same sine-wave workload; returns
-    (cell-updates/s, cores, sample description)."""
-    from oracle.oracle import Restatement  # CPU baseline leg only
+    """Times the reference's full Vlasov step (trans_map_1d_amr z, x, y, the _R
+    moments, the full acceleration step with spatial neighbours in the
+    adjustment) on a smaller periodic grid of the same sine-wave workload with
+    all host threads; returns (cell-updates/s, cores, sample description, kind)
+    or None."""
+    from oracle.oracle import ReferenceBuild, reference_available  # CPU baseline leg only
+    from vlasiator_b200.grid import grid_neighbors
     from vlasiator_b200.projects import sinewave_grid
+    if not reference_available("sp"):
+        return None
     mesh = VelocityMesh()
     cells = sinewave_grid(dims, mesh)
-    orc = Restatement("sp")
     B = np.stack([c.B for c in cells])
-    state = [(c.gids, c.data) for c in cells]
+    nbrs = grid_neighbors(dims)
+    ref = ReferenceBuild("sp")
+    ref.init(mesh)
+    cores = ref.max_threads()
+    h = ref.create([c.gids for c in cells], [c.data for c in cells], [1e-15] * len(cells))
     dt = 0.2
     updates, elapsed, steps = 0, 0.0, 0
     while elapsed < target_s and steps < 50:
-        blocks = sum(len(g) for g, _ in state)
+        blocks = sum(ref.lib.ref_cells_block_count(h, c) for c in range(len(cells)))
         t0 = time.perf_counter()
-        state, _, _, _, _ = orc.vlasov_step(mesh, dims, state, B, dt, steps % 3, (3e5, 3e5, 3e5), MASS_PROTON,
-                                            CHARGE)
+        ref.vlasov_step(h, dims, (3e5, 3e5, 3e5), B, dt, steps % 3, CHARGE, MASS_PROTON, nbrs)
         elapsed += time.perf_counter() - t0
         updates += WID3 * blocks
         steps += 1
-    return updates / elapsed, 1, (f"{dims[0]}x{dims[1]}x{dims[2]} grid of the same workload x {steps} steps "
-                                  f"({updates} cell-updates), oracle restatement, one thread")
+    ref.destroy(h)
+    return (updates / elapsed, cores,
+            f"{dims[0]}x{dims[1]}x{dims[2]} periodic grid of the same workload x {steps} full Vlasov steps "
+            f"({updates} cell-updates): the reference's trans_map_1d_amr, map_1d, adjust_velocity_blocks and "
+            f"moment templates", "reference")
 
 
 def run_reference_arm(args):
+    """The reference's own CPU code for the same workload and metric: its full
+    acceleration step (ReferenceBuild.full_step) on every cell of the
+    workload, all host threads, W untimed and K timed steps."""
     world, rank, local, pg = dist_setup()
     if rank != 0:
         return 0
@@ -231,29 +245,37 @@ def run_reference_arm(args):
     ref = ReferenceBuild("sp")
     ref.init(mesh)
     cores = ref.max_threads()
-    n = min(args.ref_sample, args.cells)
+    n = min(args.ref_sample, args.cells) if args.ref_sample > 0 else args.cells
     glist = [gids[offs[c]:offs[c + 1]] for c in range(n)]
     dlist = [data[offs[c]:offs[c + 1]] for c in range(n)]
+    total = int(offs[n])
     h = ref.create(glist, dlist, [1e-15] * n)
     for w in range(args.warmup):
-        ref.accelerate_step(h, B[:n], dt[:n], orders[w % len(orders)], CHARGE, MASS_PROTON, 0)
+        ref.full_step(h, B[:n], dt[:n], orders[w % len(orders)], CHARGE, MASS_PROTON)
     upd = 0
     t_total = 0.0
     for s in range(args.steps):
         blocks = sum(ref.lib.ref_cells_block_count(h, c) for c in range(n))
         t0 = time.perf_counter()
-        ref.accelerate_step(h, B[:n], dt[:n], orders[s], CHARGE, MASS_PROTON, 0)
+        ref.full_step(h, B[:n], dt[:n], orders[s], CHARGE, MASS_PROTON)
         t_total += time.perf_counter() - t0
         upd += WID3 * blocks
     ref.destroy(h)
     rate = upd / t_total
+    config = {"workload": WORKLOAD, "cells_per_gpu": args.cells, "blocks_per_gpu": total,
+              "mean_blocks_per_cell": total / n, "l2": "inputs larger than L2 (126 MB)",
+              "parallelism": "host threads (OpenMP over cells, as cpu_accelerate_cells)"}
+    if n < args.cells:
+        config["sampled_cells"] = n
     line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_total / max(args.steps, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": args.cells, "sampled_cells": n},
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded drifting Maxwellians)",
+            "config": config,
             "impl": "reference",
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"first {n} of the {args.cells} cells, {args.steps} steps"},
+                             "sample": (f"{'all' if n == args.cells else f'the first {n} of the'} {args.cells} "
+                                        f"cells, {args.steps} full acceleration steps (map_1d x3, "
+                                        f"adjust_velocity_blocks, moments)")},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -536,7 +558,7 @@ def run_vlasov(args):
     batch.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_vlasov_rate((8, 4, 2))
+        cpu = cpu_vlasov_rate((16, 16, 8))
     if rank != 0:
         return 0
     line = {
@@ -564,8 +586,8 @@ def run_vlasov(args):
         "clocks": clk.summary(),
     }
     if cpu is not None:
-        rate, cores, sample = cpu
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        rate, cores, sample, kind = cpu
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
     print(json.dumps(line))
     return 0
 
@@ -646,11 +668,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=4096)
-    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--seed", type=int, default=DEFAULT_SEED)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-chunks", type=int, default=32, help="accel e2e: batches the cells are split into")
-    ap.add_argument("--cpu-sample", type=int, default=256)
-    ap.add_argument("--ref-sample", type=int, default=256)
+    ap.add_argument("--cpu-sample", type=int, default=4096, help="cpu_baseline: cells timed (default all)")
+    ap.add_argument("--ref-sample", type=int, default=0, help="reference arm: cells timed (0: all)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--exact", action="store_true", help="remap in the reference's exact operation order")
     ap.add_argument("--plain-steps", type=int, default=2, help="steps of the plain per-cell path (0: skip)")

@@ -290,6 +290,11 @@ class ReferenceBuild:
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
         L.ref_cells_max_r_dt.restype = ctypes.c_double
         L.ref_cells_max_r_dt.argtypes = [_vp, _dp, _dp]
+        L.ref_cells_full_step.argtypes = [_vp, _dp, _dp, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32, ctypes.c_int, _dp]
+        L.ref_cells_vlasov_step.argtypes = [_vp, _u32p, _dp, _dp, ctypes.c_double, ctypes.c_uint32, ctypes.c_double,
+                                            ctypes.c_double, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32,
+                                            ctypes.c_int]
         L.ref_map_order.restype = ctypes.c_uint32
         L.ref_map_order.argtypes = [ctypes.c_uint32]
         L.ref_cells_content.restype = ctypes.c_uint64
@@ -377,6 +382,36 @@ class ReferenceBuild:
         d = np.ascontiguousarray(dx, np.float64)
         total = self.lib.ref_cells_max_r_dt(h, _ptr(d, ctypes.c_double), _ptr(out, ctypes.c_double))
         return out, total
+
+    def full_step(self, h, B, dt, map_order, charge, mass, neighbors=None, nthreads=0, moments=False):
+        """calculateAcceleration for one population and one subcycle on every
+        cell: pivot moments, geometry, map_1d x3, adjustVelocityBlocks (with the
+        given NEAREST neighbours, or none) and the moments with pressure.
+        Returns (n_cells, 10) moments (n, nV, sum f (v-V)(v-V)) if asked."""
+        B = np.ascontiguousarray(B, np.float64)
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (len(B),)))
+        nb, k = self._neighbors(neighbors)
+        out = np.zeros((len(B), 10)) if moments else None
+        self.lib.ref_cells_full_step(h, _ptr(B, ctypes.c_double), _ptr(dt, ctypes.c_double), map_order, charge,
+                                     mass, nb, k, nthreads, None if out is None else _ptr(out, ctypes.c_double))
+        return out
+
+    def vlasov_step(self, h, grid, dx, B, dt, map_order, charge, mass, neighbors, nthreads=0):
+        """One full Vlasov step of the periodic grid: translation z, x, y, the _R
+        moments, then full_step with the spatial neighbours."""
+        g = np.ascontiguousarray(grid, np.uint32)
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dx, np.float64), (3,)))
+        B = np.ascontiguousarray(B, np.float64)
+        nb, k = self._neighbors(neighbors)
+        self.lib.ref_cells_vlasov_step(h, _ptr(g, ctypes.c_uint32), _ptr(d, ctypes.c_double),
+                                       _ptr(B, ctypes.c_double), float(dt), map_order, charge, mass, nb, k,
+                                       nthreads)
+
+    def _neighbors(self, neighbors):
+        if neighbors is None:
+            return None, 0
+        self._nbr = np.ascontiguousarray(neighbors, np.int32)
+        return _ptr(self._nbr, ctypes.c_int32), self._nbr.shape[1]
 
     def map_order(self, tstep: int) -> int:
         """The dimension order the reference draws for time step tstep (vlasovmover.cpp:422-426)."""

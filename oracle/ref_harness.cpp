@@ -244,15 +244,7 @@ void ref_cells_accelerate_step(void* h, const double* B, const double* dt, uint3
 // spatial neighbours).  The species' minValue and blockAddWidthV are set from
 // min_value and add_width; rho_loss gets each cell's RHOLOSSADJUST added by
 // this call.
-void ref_cells_adjust(void* h, const int32_t* neighbors, uint32_t n_per_cell, double min_value, int add_width,
-                      int conserve_mass, int nthreads, double* rho_loss) {
-   RefCells* rc = (RefCells*)h;
-   if (nthreads > 0) omp_set_num_threads(nthreads);
-   species::Species& sp = getObjectWrapper().particleSpecies[0];
-   sp.sparseMinValue = min_value;
-   sp.sparseBlockAddWidthV = add_width;
-   sp.sparse_conserve_mass = conserve_mass != 0;
-   sp.sparseDynamicAlgorithm = 0;
+static void adjust_cells(RefCells* rc, const int32_t* neighbors, uint32_t n_per_cell, double* rho_loss) {
    dccrg::Dccrg<SpatialCell, dccrg::Cartesian_Geometry> g;
    std::vector<CellID> cells;
    std::vector<double> before(rc->cells.size());
@@ -270,7 +262,45 @@ void ref_cells_adjust(void* h, const int32_t* neighbors, uint32_t n_per_cell, do
    }
    spatial_cell::update_velocity_block_content_lists(g, cells, 0);
    spatial_cell::adjust_velocity_blocks_in_cells(g, cells, 0);
-   for (size_t c = 0; c < rc->cells.size(); ++c) rho_loss[c] = rc->cells[c]->populations[0].RHOLOSSADJUST - before[c];
+   if (rho_loss)
+      for (size_t c = 0; c < rc->cells.size(); ++c)
+         rho_loss[c] = rc->cells[c]->populations[0].RHOLOSSADJUST - before[c];
+}
+
+void ref_cells_adjust(void* h, const int32_t* neighbors, uint32_t n_per_cell, double min_value, int add_width,
+                      int conserve_mass, int nthreads, double* rho_loss) {
+   RefCells* rc = (RefCells*)h;
+   if (nthreads > 0) omp_set_num_threads(nthreads);
+   species::Species& sp = getObjectWrapper().particleSpecies[0];
+   sp.sparseMinValue = min_value;
+   sp.sparseBlockAddWidthV = add_width;
+   sp.sparse_conserve_mass = conserve_mass != 0;
+   sp.sparseDynamicAlgorithm = 0;
+   adjust_cells(rc, neighbors, n_per_cell, rho_loss);
+}
+
+// First moments and, about the bulk velocity, second moments of every cell
+// with the reference's reduction templates (arch_moments.h:83-155), as
+// calculateMoments_V(..., computeSecond=true) forms them; out: 10 per cell
+// (n, n V (3), sum f (v - V)_a (v - V)_b (6)); may be null (timing only).
+static void moments_cells(RefCells* rc, double* out) {
+#pragma omp parallel for schedule(dynamic, 4)
+   for (size_t c = 0; c < rc->cells.size(); ++c) {
+      SpatialCell* sc = rc->cells[c];
+      const uint n = sc->get_velocity_mesh(0)->size();
+      Real a1[4] = {0, 0, 0, 0};
+      Real a2[6] = {0, 0, 0, 0, 0, 0};
+      if (n > 0) {
+         blockVelocityFirstMoments(sc->get_velocity_blocks(0), a1, n);
+         const Real V[3] = {a1[0] != 0 ? a1[1] / a1[0] : 0, a1[0] != 0 ? a1[2] / a1[0] : 0,
+                            a1[0] != 0 ? a1[3] / a1[0] : 0};
+         blockVelocitySecondMoments(sc->get_velocity_blocks(0), V[0], V[1], V[2], a2, n);
+      }
+      if (out) {
+         for (int i = 0; i < 4; ++i) out[10 * c + i] = a1[i];
+         for (int i = 0; i < 6; ++i) out[10 * c + 4 + i] = a2[i];
+      }
+   }
 }
 
 // The content flag of every block of cell c in local-ID order, as the
@@ -316,6 +346,38 @@ uint32_t ref_map_order(uint32_t tstep) {
    std::default_random_engine rndState;
    rndState.seed(tstep);
    return (uint32_t)std::uniform_int_distribution<>(0, 2)(rndState);
+}
+
+// One full acceleration step of every cell of the set, the body of
+// calculateAcceleration for one population and one subcycle
+// (vlasovsolver/vlasovmover.cpp:410-475, 564-569): pivot moments, geometry and
+// map_1d x3 (ref_cells_accelerate_step), then adjustVelocityBlocks
+// (grid.cpp:775-817: content lists of all cells, then each cell with the
+// NEAREST neighbours given in `neighbors`, n_per_cell per cell, or none), then
+// calculateMoments_V with the second moments.  moments_out: 10 per cell or null.
+void ref_cells_full_step(void* h, const double* B, const double* dt, uint32_t map_order, double charge, double mass,
+                         const int32_t* neighbors, uint32_t n_per_cell, int nthreads, double* moments_out) {
+   RefCells* rc = (RefCells*)h;
+   ref_cells_accelerate_step(h, B, dt, map_order, charge, mass, nthreads);
+   adjust_cells(rc, neighbors, n_per_cell, nullptr);
+   moments_cells(rc, moments_out);
+}
+
+void ref_cells_translate(void* h, const uint32_t grid[3], uint32_t dimension, double dt, double dz, int nthreads);
+
+// One full Vlasov step of a uniform periodic grid (cells x fastest) in the
+// reference's main-loop order: calculateSpatialTranslation (trans_map_1d_amr
+// along z, x, y, vlasovmover.cpp:65-381) and the "_R" moments, then the full
+// acceleration step above with the spatial neighbours in the adjustment.
+void ref_cells_vlasov_step(void* h, const uint32_t grid[3], const double dx[3], const double* B, double dt,
+                           uint32_t map_order, double charge, double mass, const int32_t* neighbors,
+                           uint32_t n_per_cell, int nthreads) {
+   RefCells* rc = (RefCells*)h;
+   static const uint32_t dims[3] = {2, 0, 1};
+   for (uint32_t q = 0; q < 3; ++q) ref_cells_translate(h, grid, dims[q], dt, dx[dims[q]], nthreads);
+   moments_cells(rc, nullptr);
+   std::vector<double> dts(rc->cells.size(), dt);
+   ref_cells_full_step(h, B, dts.data(), map_order, charge, mass, neighbors, n_per_cell, nthreads, nullptr);
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }

@@ -100,3 +100,53 @@ def test_grid_adjust_matches_reference(mesh, orc_sp):
     finally:
         ref.destroy(h)
 
+
+
+def test_reference_full_step_matches_restatement(mesh, orc_sp):
+    """The reference arm's full acceleration step (pivot moments, geometry,
+    map_1d x3, adjust, moments) gives the restated step's cells and moments."""
+    from vlasiator_b200.mesh import CHARGE, MASS_PROTON
+    cells = random_drifting_cells(6, seed=12, mesh=mesh)
+    B = np.stack([c.B for c in cells])
+    dt = 0.01 * 2 * np.pi * MASS_PROTON / (CHARGE * np.linalg.norm(B, axis=1))
+    ref = ReferenceBuild("sp")
+    ref.init(mesh)
+    h = ref.create([c.gids for c in cells], [c.data for c in cells], [1e-15] * len(cells))
+    try:
+        mom = ref.full_step(h, B, dt, 2, CHARGE, MASS_PROTON, moments=True)
+        for ci, c in enumerate(cells):
+            g, d, _, _, m, _ = orc_sp.accelerate_step(mesh, c.gids, c.data, c.B, dt[ci], 2, MASS_PROTON, CHARGE)
+            gr, dr = ref.extract(h, ci)
+            np.testing.assert_array_equal(gr, g)
+            np.testing.assert_array_equal(dr, d)
+            assert mom[ci, 0] == pytest.approx(m[0], rel=1e-12)
+            np.testing.assert_allclose(mom[ci, 1:4] / mom[ci, 0], m[5:8], rtol=1e-9, atol=1e-6)
+            np.testing.assert_allclose(MASS_PROTON * mom[ci, 4:10], m[9:15], rtol=1e-9,
+                                       atol=1e-9 * np.abs(m[9:12]).max())
+    finally:
+        ref.destroy(h)
+
+
+def test_reference_vlasov_step_matches_restatement(mesh, orc_sp):
+    """The reference arm's Vlasov step of a periodic grid (translation z, x, y,
+    then the full acceleration step with spatial neighbours in the
+    adjustment) gives the restated composition's cells."""
+    from vlasiator_b200.mesh import CHARGE, MASS_PROTON
+    from vlasiator_b200.projects import sinewave_grid
+    dims = (4, 3, 2)
+    cells = sinewave_grid(dims, mesh)
+    B = np.stack([c.B for c in cells])
+    dt, mo, dx = 0.2, 1, (3e5, 3e5, 3e5)
+    ref = ReferenceBuild("sp")
+    ref.init(mesh)
+    h = ref.create([c.gids for c in cells], [c.data for c in cells], [1e-15] * len(cells))
+    try:
+        ref.vlasov_step(h, dims, dx, B, dt, mo, CHARGE, MASS_PROTON, grid_neighbors(dims))
+        want, *_ = orc_sp.vlasov_step(mesh, dims, [(c.gids, c.data) for c in cells], B, dt, mo, dx, MASS_PROTON,
+                                      CHARGE)
+        for ci in range(len(cells)):
+            gr, dr = ref.extract(h, ci)
+            np.testing.assert_array_equal(gr, want[ci][0])
+            np.testing.assert_array_equal(dr, want[ci][1])
+    finally:
+        ref.destroy(h)
