@@ -9,6 +9,8 @@
 #   oracle/_ref/libvlasov_ref_sp.so  : FP32 VDF (Realf=float, Real=double), VECL=16, PPM
 #   oracle/_ref/libvlasov_ref_dp.so  : all-FP64 (Realf=double), VECL=8, PPM
 #   oracle/_ref/libvlasov_ref_sp_pqm.so, libvlasov_ref_sp_plm.so : FP32, PQM / PLM acceleration
+#   oracle/_ref/libvlasov_ref_sp_dropin.so : the FP32 build plus the C++ drop-in layer
+#                                           (include/vlgpu.hpp) over libvlgpu.so, for its tests
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default $VLASIATOR_REF, else /root/reference)
 set -euo pipefail
@@ -90,6 +92,15 @@ pids=()
   -o "$OUT/libvlasov_ref_sp_pqm.so" & pids+=($!)
 "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PLM -DSPF -DVECL=16 "${SRCS[@]}" "$OUT/orc_geometry_sp.o" \
   -o "$OUT/libvlasov_ref_sp_plm.so" & pids+=($!)
+# the C++ drop-in layer (include/vlgpu.hpp) instantiated with the stand-in
+# cell beside the reference's own map_1d, linked against libvlgpu.so
+LIBVLGPU="$HERE/../vlasiator_b200/libvlgpu.so"
+cp "$HERE/dropin_harness.cpp" "$SRC/dropin_harness.cpp"
+if [ -f "$LIBVLGPU" ]; then
+  "$CXX" "${COMMON[@]}" -DACC_SEMILAG_PPM -DSPF -DVECL=16 -I"$HERE/../include" "${SRCS[@]}" "$SRC/dropin_harness.cpp" \
+    "$OUT/orc_geometry_sp.o" -L"$HERE/../vlasiator_b200" -lvlgpu -Wl,-rpath,'$ORIGIN/../../vlasiator_b200' \
+    -o "$OUT/libvlasov_ref_sp_dropin.so" & pids+=($!)
+fi
 fail=0
 for p in "${pids[@]}"; do wait "$p" || fail=1; done
 if [ "$fail" -ne 0 ]; then echo "build_ref: a compilation failed" >&2; exit 4; fi

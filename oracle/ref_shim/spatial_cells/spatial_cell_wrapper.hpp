@@ -36,6 +36,10 @@ struct Population {
    Real RHOLOSSADJUST{0};
    Real RHO{0};
    Real max_dt[2]{0, 0};  // species::MAXRDT, species::MAXVDT
+   Real intersection_x{0}, intersection_x_di{0}, intersection_x_dj{0}, intersection_x_dk{0};
+   Real intersection_y{0}, intersection_y_di{0}, intersection_y_dj{0}, intersection_y_dk{0};
+   Real intersection_z{0}, intersection_z_di{0}, intersection_z_dj{0}, intersection_z_dk{0};
+   Real subcycleDt{0};
    Population() {
       vmesh = new vmesh::VelocityMesh();
       blockContainer = new vmesh::VelocityBlockContainer();
@@ -51,6 +55,7 @@ struct Population {
 class SpatialCell {
  public:
    Real parameters[CellParams::N_SPATIAL_CELL_PARAMS];
+   std::array<Real, bvolderivatives::N_BVOL_DERIVATIVES> derivativesBVOL{};
    std::deque<Population> populations;
    std::vector<vmesh::GlobalID>* velocity_block_with_content_list;
    std::vector<vmesh::GlobalID>* velocity_block_with_no_content_list;
