@@ -45,11 +45,13 @@ struct CellAccelInputs {
 cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
                            double* moments, const double* shift, const MeshDev& mesh, const double vmin[3],
                            const double bs[3], const double dv[3], double mass, double charge, bool second,
-                           uint32_t n_cells, cudaStream_t stream);
+                           uint32_t n_cells, double* part_sums, uint32_t* done, int grid, cudaStream_t stream);
 cudaError_t launch_moments_both(const uint32_t* gids, const uint32_t* src_index, const float* data,
                                 const CellSlot* slots, double* pivot, double* moments, const MeshDev& mesh,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
-                                double charge, uint32_t n_cells, cudaStream_t stream);
+                                double charge, uint32_t n_cells, double* part_sums, uint32_t* done, int grid,
+                                cudaStream_t stream);
+int moments_blocks_per_sm();
 cudaError_t launch_geometry(const CellAccelInputs* in, const double* moments, double* isect12, SweepCell* sweep3,
                             uint32_t n_cells, double q, double m, double hall_min_rhoq, int ohm_gradpe, double mu0,
                             const double vmin[3], const double dv[3], uint32_t map_order, float threshold,
@@ -150,6 +152,9 @@ struct vlgpu_batch {
    CellAccelInputs* accel_in = nullptr;
    double* moments = nullptr;  // MOM_COUNT per cell
    double* pivot = nullptr;    // MOM_COUNT per cell: first moments (U = 0) the acceleration transform uses
+   double* mom_parts = nullptr;   // per cell and part, the part's sums (moments work array)
+   uint32_t* mom_done = nullptr;  // per cell, the parts finished (zero between passes)
+   int mom_grid = 0;
    double* isect12 = nullptr;  // 12 per cell
    double* loss = nullptr;     // RHOLOSSADJUST per cell
    uint32_t* status = nullptr;

@@ -32,6 +32,8 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->accel_in);
    cudaFree(b->moments);
    cudaFree(b->pivot);
+   cudaFree(b->mom_parts);
+   cudaFree(b->mom_done);
    cudaFree(b->isect12);
    cudaFree(b->loss);
    cudaFree(b->status);
@@ -133,7 +135,7 @@ int moments_device(vlgpu_batch* b, bool second, double* record, const double* sh
    b->launches += 1;
    VL_CHECK(launch_moments(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, record ? record : b->moments, shift,
                            b->mdev, b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, second,
-                           b->n_cells, b->stream));
+                           b->n_cells, b->mom_parts, b->mom_done, b->mom_grid, b->stream));
    return VLGPU_OK;
 }
 
@@ -144,7 +146,7 @@ int moments_both_device(vlgpu_batch* b, double* record) {
    b->launches += 1;
    VL_CHECK(launch_moments_both(b->st_gids, b->st_src, b->data[b->cur], b->st_slots, b->pivot, record, b->mdev,
                                 b->vmin_d, b->bs_d, b->dv_d, b->params.mass, b->params.charge, b->n_cells,
-                                b->stream));
+                                b->mom_parts, b->mom_done, b->mom_grid, b->stream));
    b->pivot_valid = true;
    return VLGPU_OK;
 }
@@ -350,6 +352,7 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
    b->remap_grid = b->sm_count * remap_blocks_per_sm();
    b->adj_grid = b->sm_count * adjust_blocks_per_sm();
+   b->mom_grid = b->sm_count * moments_blocks_per_sm();
    const uint64_t cap = block_capacity;
    for (int p = 0; p < 2; ++p) {
       if ((e = cudaMalloc(&b->gids[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "gids");
@@ -371,6 +374,11 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMemset(b->moments, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMalloc(&b->pivot, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMemset(b->pivot, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMalloc(&b->mom_parts, sizeof(double) * MOM_SUMS_PER_PART * MOM_PARTS_PER_CELL * n_cells)) !=
+       cudaSuccess)
+      return fail(e, "mom");
+   if ((e = cudaMalloc(&b->mom_done, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMemset(b->mom_done, 0, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMalloc(&b->isect12, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
    if ((e = cudaMemset(b->isect12, 0, sizeof(double) * 12 * n_cells)) != cudaSuccess) return fail(e, "isect");
    if ((e = cudaMalloc(&b->loss, sizeof(double) * n_cells)) != cudaSuccess) return fail(e, "loss");
@@ -378,6 +386,8 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMalloc(&b->status, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "status");
    if ((e = cudaMemset(b->status, 0, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "status");
    if ((e = cudaMalloc(&b->counters, sizeof(SweepCounters))) != cudaSuccess) return fail(e, "counters");
+   // no sweep has run: vlgpu_batch_sync reads the overflow flag from here
+   if ((e = cudaMemset(b->counters, 0, sizeof(SweepCounters))) != cudaSuccess) return fail(e, "counters");
    if ((e = cudaMalloc(&b->stats, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMalloc(&b->rows_used, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMalloc(&b->adj_scratch, sizeof(uint32_t) * adjust_scratch_words(b->mdev) *

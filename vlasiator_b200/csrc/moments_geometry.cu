@@ -1,15 +1,15 @@
-// Velocity moments (FP64, Kahan-compensated) and the per-cell FP64
-// acceleration geometry, for sm_100a.
+// Velocity moments (FP64, compensated) and the per-cell FP64 acceleration
+// geometry, for sm_100a.
 //
-// moments_kernel: one CTA per cell, one pass over the cell's data.  Sixteen
-// threads share a velocity block, each reading one x-row of four cells as a
-// float4, with several blocks in flight per thread group; per-thread partial
-// sums are Kahan-compensated doubles, merged across the CTA with error-free
-// (TwoSum) additions.  The sums are those of blockVelocityFirstMoments /
+// moments_parts_kernel: every cell's blocks in up to 64 equal parts, each
+// part summed by one warp (half a warp per velocity block, one float4 x-row
+// of four cells per lane) with FP64 arithmetic, the parts of a cell added in
+// part order with compensated sums by whichever warp finishes the cell's last
+// part.  The sums are those of blockVelocityFirstMoments /
 // blockVelocitySecondMoments (vlasovsolver/arch_moments.h:83-155) and the
 // per-cell bookkeeping of calculateMoments_V
 // (vlasovsolver/arch_moments.cpp:342-499); the pressure tensor comes from
-// velocities taken relative to the previous bulk velocity (see the kernel).
+// velocities taken relative to an earlier bulk velocity (see the kernel).
 //
 // geometry_kernel: one thread per cell builds the gyration transform and the
 // three intersection sets in FP64 (geometry.cuh) and converts them into the
@@ -42,230 +42,72 @@ enum MomentSlot {
    MOM_COUNT = 16
 };
 
-struct Kahan {
-   double s = 0.0, c = 0.0;
-   __device__ __forceinline__ void add(double x) {
-      const double y = x - c;
-      const double t = s + y;
-      c = (t - s) - y;
-      s = t;
-   }
-};
-
-// error-free merge of two compensated sums (Knuth TwoSum on the heads)
-__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
-   const double s = hi + bhi;
-   const double bb = s - hi;
-   const double err = (hi - (s - bb)) + (bhi - bb);
-   hi = s;
-   lo = lo + blo + err;
-}
-
-constexpr int MOM_THREADS = 256;
-constexpr int MOM_GROUPS = MOM_THREADS / 16;  // 16 threads per velocity block
-constexpr int MOM_MAXSUMS = 10;
-
-template <int N>
-__device__ __forceinline__ void cta_reduce(double hi[N], double lo[N], double* sh_hi, double* sh_lo) {
-   // warp level
-#pragma unroll
-   for (int q = 0; q < N; ++q) {
-#pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) {
-         const double oh = __shfl_xor_sync(0xffffffffu, hi[q], o);
-         const double ol = __shfl_xor_sync(0xffffffffu, lo[q], o);
-         dd_add(hi[q], lo[q], oh, ol);
-      }
-   }
-   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   if (lane == 0)
-      for (int q = 0; q < N; ++q) {
-         sh_hi[warp * N + q] = hi[q];
-         sh_lo[warp * N + q] = lo[q];
-      }
-   __syncthreads();
-   if (threadIdx.x == 0) {
-      for (int q = 0; q < N; ++q) {
-         double h = 0.0, l = 0.0;
-         for (int w = 0; w < MOM_THREADS / 32; ++w) dd_add(h, l, sh_hi[w * N + q], sh_lo[w * N + q]);
-         hi[q] = h;
-         lo[q] = l;
-      }
-   }
-   __syncthreads();
-}
-
-// One CTA per cell; 16 threads per velocity block, each owning one x-row of
-// four cells (a float4: i = 0..3 at j = sub & 3, k = sub >> 2), and every
-// thread group keeps MOM_UNROLL blocks in flight.  With SECOND, velocities
-// are taken relative to a reference velocity U (a bulk velocity of an
-// earlier VDF of the cell: the acceleration step's pivot), so one pass over
-// the data gives both the first moments and the central second moments:
-//   S0 = sum f, S_a = sum f u_a, S_ab = sum f u_a u_b   (u = v - U)
+// Each cell's blocks are split into equal parts of at least 32 blocks (at
+// most MOM_PARTS_PER_CELL parts); a warp takes (part, cell) items in a fixed
+// grid-stride order (consecutive items are the same part of consecutive
+// cells, so the work of large and small cells interleaves), sums its part
+// with FP64 arithmetic per lane, adds the lanes' sums in lane order, and
+// stores the part's sums.  Per lane and block the four cells of a row enter
+// as the row's sums of f, i f and i^2 f (i = 0..3), combined with the row's
+// first cell centre.  The last
+// part of a cell to finish (a per-cell counter) adds the cell's parts in part
+// order with compensated sums and writes the record, so the result does not
+// depend on which warp ran which part.  Half a warp reads one velocity block,
+// each lane one x-row of four cells as a float4 (i = 0..3 at j = sub & 3,
+// k = sub >> 2), two blocks per half-warp in flight.
+//
+// The sums are those of blockVelocityFirstMoments / blockVelocitySecondMoments
+// (vlasovsolver/arch_moments.h:83-155) and the record that of
+// calculateMoments_V (vlasovsolver/arch_moments.cpp:342-499).  With velocities
+// taken relative to a reference velocity U (u = v - U):
+//   S0 = sum f, S_a = sum f u_a, S_ab = sum f u_a u_b,
 //   n V_a = (S_a + U_a S0) dv^3,  P_ab = m dv^3 (S_ab - S_a S_b / S0).
-// With U close to V the correction term is small, so nothing cancels; the
-// result equals the reference's two-pass sums (first V, then f (v-V)(v-V))
-// up to FP64 rounding.  Without SECOND, U = 0, so the first moments depend
-// on the data alone.
+// With U close to the bulk velocity nothing cancels, and the result equals the
+// reference's two-pass sums (first V, then f (v-V)(v-V)) up to FP64 rounding.
 //
-// moments_pass is one such pass of a CTA over one cell's blocks; thread 0
-// writes the cell's record `out`.
-//
-// MODE MOM_BOTH does the work of a first-moments pass and a second-moments
-// pass in one read: the first sums with U = 0 (the same arithmetic as
-// MOM_FIRST, so the first moments are identical) and the second sums about
-// the U given, whose first sums T_a = S_a - U_a S0 follow from the former;
-// the cancellation in T_a costs about eps (U / v_th)^2 of P relative, far
-// below the tolerance of any use, and vanishes as U approaches V.  It writes
-// the first moments to `out1` (pressure zero, as MOM_FIRST) and everything
-// to `out`.
+// Modes: MOM_FIRST sums the first moments about 0; MOM_SECOND sums everything
+// about the U of the `shift` record; MOM_BOTH does both passes' work in one
+// read: the first sums about 0 with exactly MOM_FIRST's arithmetic (so the
+// first moments, which the next acceleration takes as its pivot, are
+// bit-identical to a MOM_FIRST pass) and the second sums about the U of the
+// pivot record, whose first sums T_a = S_a - U_a S0 follow from the former;
+// the cancellation in T_a costs about eps (U / v_th)^2 of P relative and
+// vanishes as U approaches V.  MOM_BOTH writes the full record to `out` and
+// the first moments (pressure zero, as MOM_FIRST) to the pivot record.
 constexpr int MOM_FIRST = 0, MOM_SECOND = 1, MOM_BOTH = 2;
+constexpr int MOM_THREADS = 256;
 
+// The record of a cell from its sums S (about U for the second moments; the
+// first sums about F, which is 0 or U).
 template <int MODE>
-__device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index,
-                                             const float* __restrict__ data, const CellSlot s, double* out,
-                                             const MeshDev& mesh, double vmin0, double vmin1, double vmin2, double bs0,
-                                             double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-                                             double charge, double U0, double U1, double U2, double* sh_hi,
-                                             double* sh_lo, double* out1 = nullptr) {
+__device__ __forceinline__ void moments_record(const double* S, double F0, double F1, double F2, double U0, double U1,
+                                            double U2, double dv0, double dv1, double dv2, double mass, double charge,
+                                            double* out, double* out1) {
    constexpr bool SECOND = MODE != MOM_FIRST;
-   constexpr int NS = SECOND ? 10 : 4;
-   const int sub = threadIdx.x & 15, grp = threadIdx.x >> 4;
-   const int j = sub & 3, k = sub >> 2;
-   // velocity offsets of the first sums (U = 0 in MOM_BOTH) and of the second
-   const double F0 = (MODE == MOM_BOTH) ? 0.0 : U0, F1 = (MODE == MOM_BOTH) ? 0.0 : U1;
-   const double F2 = (MODE == MOM_BOTH) ? 0.0 : U2;
-   const double cy = (j + 0.5) * dv1 - F1, cz = (k + 0.5) * dv2 - F2;
-   const double cx0 = 0.5 * dv0 - F0, cx1 = 1.5 * dv0 - F0, cx2 = 2.5 * dv0 - F0, cx3 = 3.5 * dv0 - F0;
-   const double sy = (j + 0.5) * dv1 - U1, sz = (k + 0.5) * dv2 - U2;
-   const double sx0 = 0.5 * dv0 - U0, sx1 = 1.5 * dv0 - U0, sx2 = 2.5 * dv0 - U0, sx3 = 3.5 * dv0 - U0;
-   Kahan acc[NS];
-   constexpr int MOM_UNROLL = (MODE == MOM_FIRST) ? 8 : (MODE == MOM_SECOND ? 4 : 2);  // blocks in flight per group
-   constexpr uint32_t STEP = MOM_GROUPS * MOM_UNROLL;
-   // block IDs and data indices of a batch; the next batch's are loaded while
-   // the current batch's data is in flight, so a batch waits on one round
-   // trip to memory, not on the index lookup before it
-   uint32_t g[MOM_UNROLL], idx[MOM_UNROLL];
-   auto fetch = [&](uint32_t b0, uint32_t* gg, uint32_t* ii) {
-#pragma unroll
-      for (int u = 0; u < MOM_UNROLL; ++u) {
-         const uint32_t b = b0 + u * MOM_GROUPS;
-         gg[u] = (b < s.count) ? __ldg(gids + s.off + b) : 0u;
-         ii[u] = (b < s.count) ? (src_index ? __ldg(src_index + s.off + b) : s.off + b) : 0xffffffffu;
-      }
-   };
-   fetch(grp, g, idx);
-   // per-thread sums of a batch, added to the compensated sums once per
-   // batch; in MOM_BOTH the first sums keep MOM_FIRST's batches of 8 blocks
-   // (four of its batches of 2, same blocks in the same order), so that its
-   // first moments are bit-identical to a MOM_FIRST pass
-   double t[NS];
-#pragma unroll
-   for (int q = 0; q < NS; ++q) t[q] = 0.0;
-   int vb = 0;
-   for (uint32_t b0 = grp; b0 < s.count; b0 += STEP) {
-      float4 f4[MOM_UNROLL];
-#pragma unroll
-      for (int u = 0; u < MOM_UNROLL; ++u) {
-         f4[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-         if (idx[u] != 0xffffffffu)  // an added block holds zeros
-            f4[u] = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx[u] * WID3) + sub);
-      }
-      uint32_t g_next[MOM_UNROLL], idx_next[MOM_UNROLL];
-      fetch(b0 + STEP, g_next, idx_next);
-#pragma unroll
-      for (int u = 0; u < MOM_UNROLL; ++u) {
-         uint32_t bi, bj, bk;
-         block_xyz(mesh, g[u], bi, bj, bk);
-         const double bx = vmin0 + bi * bs0;
-         const double uy = (vmin1 + bj * bs1) + cy;
-         const double uz = (vmin2 + bk * bs2) + cz;
-         const double x0 = bx + cx0, x1 = bx + cx1, x2 = bx + cx2, x3 = bx + cx3;
-         const double f0 = f4[u].x, f1 = f4[u].y, f2 = f4[u].z, f3 = f4[u].w;
-         const double sf = (f0 + f1) + (f2 + f3);
-         const double fx0 = f0 * x0, fx1 = f1 * x1, fx2 = f2 * x2, fx3 = f3 * x3;
-         const double sfx = (fx0 + fx1) + (fx2 + fx3);
-         t[0] += sf;
-         t[1] += sfx;
-         t[2] += sf * uy;
-         t[3] += sf * uz;
-         if constexpr (MODE == MOM_SECOND) {
-            t[4] += (fx0 * x0 + fx1 * x1) + (fx2 * x2 + fx3 * x3);
-            t[5] += sf * uy * uy;
-            t[6] += sf * uz * uz;
-            t[7] += sf * uy * uz;
-            t[8] += sfx * uz;
-            t[9] += sfx * uy;
-         }
-         if constexpr (MODE == MOM_BOTH) {
-            const double vy = (vmin1 + bj * bs1) + sy, vz = (vmin2 + bk * bs2) + sz;
-            const double y0 = bx + sx0, y1 = bx + sx1, y2 = bx + sx2, y3 = bx + sx3;
-            const double fy0 = f0 * y0, fy1 = f1 * y1, fy2 = f2 * y2, fy3 = f3 * y3;
-            const double sfy = (fy0 + fy1) + (fy2 + fy3);
-            t[4] += (fy0 * y0 + fy1 * y1) + (fy2 * y2 + fy3 * y3);
-            t[5] += sf * vy * vy;
-            t[6] += sf * vz * vz;
-            t[7] += sf * vy * vz;
-            t[8] += sfy * vz;
-            t[9] += sfy * vy;
-         }
-      }
-      if constexpr (MODE == MOM_BOTH) {
-#pragma unroll
-         for (int q = 4; q < NS; ++q) {
-            acc[q].add(t[q]);
-            t[q] = 0.0;
-         }
-         if (++vb == 4) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-               acc[q].add(t[q]);
-               t[q] = 0.0;
-            }
-            vb = 0;
-         }
-      } else {
-#pragma unroll
-         for (int q = 0; q < NS; ++q) {
-            acc[q].add(t[q]);
-            t[q] = 0.0;
-         }
-      }
-#pragma unroll
-      for (int u = 0; u < MOM_UNROLL; ++u) {
-         g[u] = g_next[u];
-         idx[u] = idx_next[u];
-      }
-   }
-   if (MODE == MOM_BOTH && vb) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q].add(t[q]);
-   }
-   double hi[NS], lo[NS];
-#pragma unroll
-   for (int q = 0; q < NS; ++q) {
-      hi[q] = acc[q].s;
-      lo[q] = -acc[q].c;
-   }
-   cta_reduce<NS>(hi, lo, sh_hi, sh_lo);
-   if (threadIdx.x != 0) return;
-   double S[NS];
-#pragma unroll
-   for (int q = 0; q < NS; ++q) S[q] = hi[q] + lo[q];
    const double DV3 = dv0 * dv1 * dv2;
    const double a0 = S[0] * DV3;
    const double a1 = (S[1] + F0 * S[0]) * DV3, a2 = (S[2] + F1 * S[0]) * DV3, a3 = (S[3] + F2 * S[0]) * DV3;
-   out[MOM_N] = a0;
-   out[MOM_NVX] = a1;
-   out[MOM_NVY] = a2;
-   out[MOM_NVZ] = a3;
    const double rhom = a0 * mass;
-   out[MOM_RHOM] = rhom;
-   out[MOM_VX] = (rhom != 0.0) ? (a1 * mass) / rhom : 0.0;
-   out[MOM_VY] = (rhom != 0.0) ? (a2 * mass) / rhom : 0.0;
-   out[MOM_VZ] = (rhom != 0.0) ? (a3 * mass) / rhom : 0.0;
-   out[MOM_RHOQ] = a0 * charge;
+   const double first[MOM_P11] = {a0,
+                                  a1,
+                                  a2,
+                                  a3,
+                                  rhom,
+                                  (rhom != 0.0) ? (a1 * mass) / rhom : 0.0,
+                                  (rhom != 0.0) ? (a2 * mass) / rhom : 0.0,
+                                  (rhom != 0.0) ? (a3 * mass) / rhom : 0.0,
+                                  a0 * charge};
+#pragma unroll
+   for (int q = 0; q < MOM_P11; ++q) {
+      out[q] = first[q];
+      if (MODE == MOM_BOTH && out1) out1[q] = first[q];
+   }
    out[MOM_MASS] = S[0];
+   if (MODE == MOM_BOTH && out1) {
+      out1[MOM_MASS] = S[0];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) out1[MOM_P11 + q] = 0.0;
+   }
    double P[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
    if constexpr (SECOND) {
       if (S[0] != 0.0) {
@@ -283,28 +125,184 @@ __device__ __forceinline__ void moments_pass(const uint32_t* __restrict__ gids, 
          P[5] = pre * (S[9] - T1 * m2);
       }
    }
+#pragma unroll
    for (int q = 0; q < 6; ++q) out[MOM_P11 + q] = P[q];
-   if (MODE == MOM_BOTH && out1) {
-      for (int q = 0; q < MOM_COUNT; ++q) out1[q] = (q >= MOM_P11 && q < MOM_P11 + 6) ? 0.0 : out[q];
-   }
 }
 
-// With SECOND the reference velocity U is the bulk velocity in the cell's
-// record of `shift`.
-template <bool SECOND>
-__global__ void __launch_bounds__(MOM_THREADS, 2) moments_kernel(
+// Parts of a cell with `count` blocks: enough that a part has at least
+// MOM_MIN_PART blocks, at most MOM_PARTS_PER_CELL.
+constexpr uint32_t MOM_MIN_PART = 256;
+constexpr uint32_t MOM_TILE = 256;  // blocks of a part staged at a time
+__device__ __forceinline__ uint32_t moment_parts(uint32_t count) {
+   const uint32_t p = (count + MOM_MIN_PART - 1) / MOM_MIN_PART;
+   return p < (uint32_t)MOM_PARTS_PER_CELL ? p : (uint32_t)MOM_PARTS_PER_CELL;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(MOM_THREADS, 2) moments_parts_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
-   const CellSlot* __restrict__ slots, double* moments, const double* shift, MeshDev mesh, double vmin0,
-   double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-   double charge) {
-   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   const uint32_t cell = blockIdx.x;
-   double* out = moments + (size_t)cell * MOM_COUNT;
-   const double* sh = shift + (size_t)cell * MOM_COUNT;
-   const double U0 = SECOND ? sh[MOM_VX] : 0.0, U1 = SECOND ? sh[MOM_VY] : 0.0, U2 = SECOND ? sh[MOM_VZ] : 0.0;
-   moments_pass<SECOND ? MOM_SECOND : MOM_FIRST>(gids, src_index, data, slots[cell], out, mesh, vmin0, vmin1, vmin2,
-                                                 bs0, bs1, bs2, dv0, dv1, dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo);
+   const CellSlot* __restrict__ slots, double* moments, double* pivot, const double* shift,
+   double* __restrict__ part_sums, uint32_t* __restrict__ done, MeshDev mesh, double vmin0, double vmin1,
+   double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass, double charge,
+   uint32_t n_cells) {
+   constexpr bool SECOND = MODE != MOM_FIRST;
+   constexpr int NS = SECOND ? 10 : 4;
+   __shared__ double sh[MOM_THREADS / 32][NS][33];  // a warp's lane sums, one row per sum (padded)
+   __shared__ uint32_t sg[MOM_THREADS / 32][MOM_TILE], si[MOM_THREADS / 32][MOM_TILE];  // a tile's block IDs, rows
+   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+   const int half = lane >> 4, sub = lane & 15;
+   const int j = sub & 3, k = sub >> 2;
+   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+   const uint32_t n_items = n_cells * (uint32_t)MOM_PARTS_PER_CELL;
+   const double dv0s = dv0 * dv0;
+   for (uint32_t it = warp; it < n_items; it += n_warps) {
+      const uint32_t part = it / n_cells, cell = it - part * n_cells;
+      const CellSlot s = slots[cell];
+      const uint32_t parts = moment_parts(s.count);
+      if (parts == 0) {
+         // a cell without blocks: a zero record (and pivot)
+         if (part == 0 && lane < MOM_COUNT) {
+            moments[(size_t)cell * MOM_COUNT + lane] = 0.0;
+            if (MODE == MOM_BOTH) pivot[(size_t)cell * MOM_COUNT + lane] = 0.0;
+         }
+         continue;
+      }
+      if (part >= parts) continue;
+      const uint32_t b0 = (uint32_t)(((uint64_t)s.count * part) / parts);
+      const uint32_t b1 = (uint32_t)(((uint64_t)s.count * (part + 1)) / parts);
+      // the reference velocity: the pivot's (MOM_BOTH) or the shift record's (MOM_SECOND)
+      double U0 = 0.0, U1 = 0.0, U2 = 0.0;
+      if (MODE == MOM_BOTH) {
+         const double* pv = pivot + (size_t)cell * MOM_COUNT;
+         U0 = pv[MOM_VX]; U1 = pv[MOM_VY]; U2 = pv[MOM_VZ];
+      } else if (MODE == MOM_SECOND) {
+         const double* sh_rec = shift + (size_t)cell * MOM_COUNT;
+         U0 = sh_rec[MOM_VX]; U1 = sh_rec[MOM_VY]; U2 = sh_rec[MOM_VZ];
+      }
+      // the first sums are about F (0, or U in MOM_SECOND); a lane's row of
+      // four cells starts at the cell centre x0 = corner + dv0/2 - F0, the
+      // others follow at dv0 steps
+      const double F0 = (MODE == MOM_SECOND) ? U0 : 0.0, F1 = (MODE == MOM_SECOND) ? U1 : 0.0;
+      const double F2 = (MODE == MOM_SECOND) ? U2 : 0.0;
+      const double ox = 0.5 * dv0 - F0, oy = (j + 0.5) * dv1 - F1, oz = (k + 0.5) * dv2 - F2;
+      double t[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) t[q] = 0.0;
+      // tiles of the part: the block IDs and data rows are staged in shared
+      // memory (coalesced), then half-warp h reads blocks h, h + 2, h + 4,
+      // h + 6 of every eight, all four loads in flight at once
+      for (uint32_t t0 = b0; t0 < b1; t0 += MOM_TILE) {
+         const uint32_t n = (b1 - t0 < MOM_TILE) ? b1 - t0 : MOM_TILE;
+         for (uint32_t q = lane; q < n; q += 32) {
+            sg[wl][q] = __ldg(gids + s.off + t0 + q);
+            si[wl][q] = src_index ? __ldg(src_index + s.off + t0 + q) : s.off + t0 + q;
+         }
+         __syncwarp();
+         // rows of blocks q0 + 2u (u = 0..3) of this half-warp, the next four
+         // prefetched while these are summed
+         auto load4 = [&](uint32_t q0, float4* f) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+               const uint32_t q = q0 + 2 * u;
+               f[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+               if (q < n) {
+                  const uint32_t idx = si[wl][q];
+                  if (idx != 0xffffffffu)  // an added block holds zeros
+                     f[u] = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx * WID3) + sub);
+               }
+            }
+         };
+         float4 cur[4], nxt[4];
+         load4(half, cur);
+         for (uint32_t q0 = half; q0 < n; q0 += 8) {
+            load4(q0 + 8, nxt);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+               uint32_t bi, bj, bk;
+               block_xyz(mesh, sg[wl][(q0 + 2 * u < n) ? q0 + 2 * u : 0], bi, bj, bk);
+               // the row's sums of f, i f and i^2 f (i = 0..3 along x)
+               const double d0 = cur[u].x, d1 = cur[u].y, d2 = cur[u].z, d3 = cur[u].w;
+               const double s0 = (d0 + d1) + (d2 + d3);
+               const double s1 = fma(3.0, d3, fma(2.0, d2, d1));
+               const double s2 = fma(9.0, d3, fma(4.0, d2, d1));
+               const double x0 = (vmin0 + bi * bs0) + ox;
+               const double uy = (vmin1 + bj * bs1) + oy;
+               const double uz = (vmin2 + bk * bs2) + oz;
+               const double ds1 = dv0 * s1;
+               const double sfx = fma(x0, s0, ds1);  // sum f x over the row
+               t[0] += s0;
+               t[1] += sfx;
+               t[2] = fma(s0, uy, t[2]);
+               t[3] = fma(s0, uz, t[3]);
+               if constexpr (MODE == MOM_SECOND) {
+                  // sum f x^2 = x0^2 s0 + 2 x0 dv0 s1 + dv0^2 s2
+                  t[4] += fma(x0, fma(x0, s0, 2.0 * ds1), dv0s * s2);
+                  const double s0y = s0 * uy;
+                  t[5] = fma(s0y, uy, t[5]);
+                  t[6] = fma(s0 * uz, uz, t[6]);
+                  t[7] = fma(s0y, uz, t[7]);
+                  t[8] = fma(sfx, uz, t[8]);
+                  t[9] = fma(sfx, uy, t[9]);
+               }
+               if constexpr (MODE == MOM_BOTH) {
+                  // the same row relative to U (the first sums were about 0)
+                  const double y0 = x0 - U0, vy = uy - U1, vz = uz - U2;
+                  const double sfy = fma(y0, s0, ds1);
+                  t[4] += fma(y0, fma(y0, s0, 2.0 * ds1), dv0s * s2);
+                  const double s0y = s0 * vy;
+                  t[5] = fma(s0y, vy, t[5]);
+                  t[6] = fma(s0 * vz, vz, t[6]);
+                  t[7] = fma(s0y, vz, t[7]);
+                  t[8] = fma(sfy, vz, t[8]);
+                  t[9] = fma(sfy, vy, t[9]);
+               }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cur[u] = nxt[u];
+         }
+         __syncwarp();
+      }
+      // the part's sums: the warp's lane sums added in lane order by lanes 0..NS-1
+#pragma unroll
+      for (int q = 0; q < NS; ++q) sh[wl][q][lane] = t[q];
+      __syncwarp();
+      double* ps = part_sums + ((size_t)cell * MOM_PARTS_PER_CELL + part) * MOM_SUMS_PER_PART;
+      if (lane < NS) {
+         double v = 0.0;
+         for (int l = 0; l < 32; ++l) v += sh[wl][lane][l];
+         ps[lane] = v;
+      }
+      __syncwarp();
+      __threadfence();
+      uint32_t prev = 0;
+      if (lane == 0) prev = atomicAdd(&done[cell], 1u);
+      prev = __shfl_sync(0xffffffffu, prev, 0);
+      if (prev + 1 != parts) continue;
+      // the cell's last part: add all parts in part order
+      __threadfence();
+      double S = 0.0;
+      if (lane < NS) {
+         double sum = 0.0, comp = 0.0;
+         const double* base = part_sums + (size_t)cell * MOM_PARTS_PER_CELL * MOM_SUMS_PER_PART + lane;
+         for (uint32_t p = 0; p < parts; ++p) {
+            const double y = __ldcg(base + (size_t)p * MOM_SUMS_PER_PART) - comp;
+            const double tt = sum + y;
+            comp = (tt - sum) - y;
+            sum = tt;
+         }
+         S = sum - comp;
+      }
+      double Sv[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) Sv[q] = __shfl_sync(0xffffffffu, S, q);
+      if (lane == 0) {
+         moments_record<MODE>(Sv, F0, F1, F2, U0, U1, U2, dv0, dv1, dv2, mass, charge,
+                              moments + (size_t)cell * MOM_COUNT,
+                              MODE == MOM_BOTH ? pivot + (size_t)cell * MOM_COUNT : nullptr);
+         done[cell] = 0;  // ready for the next pass
+      }
+   }
 }
 
 // Per-cell acceleration inputs on the device.
@@ -416,49 +414,38 @@ cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const Cel
 }
 
 // ---------------------------------------------------------------------------
+int moments_blocks_per_sm() {
+   int n = 0;
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, moments_parts_kernel<MOM_BOTH>, MOM_THREADS, 0);
+   return n > 0 ? n : 1;
+}
+
 cudaError_t launch_moments(const uint32_t* gids, const uint32_t* src_index, const float* data, const CellSlot* slots,
                            double* moments, const double* shift, const MeshDev& mesh, const double vmin[3],
                            const double bs[3], const double dv[3], double mass, double charge, bool second,
-                           uint32_t n_cells, cudaStream_t stream) {
+                           uint32_t n_cells, double* part_sums, uint32_t* done, int grid, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
    if (!shift) shift = moments;
    if (second)
-      moments_kernel<true><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, shift, mesh,
-                                                               vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                               dv[1], dv[2], mass, charge);
+      moments_parts_kernel<MOM_SECOND><<<grid, MOM_THREADS, 0, stream>>>(
+         gids, src_index, data, slots, moments, nullptr, shift, part_sums, done, mesh, vmin[0], vmin[1], vmin[2],
+         bs[0], bs[1], bs[2], dv[0], dv[1], dv[2], mass, charge, n_cells);
    else
-      moments_kernel<false><<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, moments, shift, mesh,
-                                                                vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                                dv[1], dv[2], mass, charge);
+      moments_parts_kernel<MOM_FIRST><<<grid, MOM_THREADS, 0, stream>>>(
+         gids, src_index, data, slots, moments, nullptr, shift, part_sums, done, mesh, vmin[0], vmin[1], vmin[2],
+         bs[0], bs[1], bs[2], dv[0], dv[1], dv[2], mass, charge, n_cells);
    return cudaGetLastError();
-}
-
-// MOM_BOTH of every cell: reference velocity U from the cell's record in
-// `pivot`, which then receives the first moments of this VDF; the moments
-// with pressure go to `moments`.
-__global__ void __launch_bounds__(MOM_THREADS, 2) moments_both_kernel(
-   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const float* __restrict__ data,
-   const CellSlot* __restrict__ slots, double* pivot, double* __restrict__ moments, MeshDev mesh, double vmin0,
-   double vmin1, double vmin2, double bs0, double bs1, double bs2, double dv0, double dv1, double dv2, double mass,
-   double charge) {
-   __shared__ double sh_hi[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   __shared__ double sh_lo[(MOM_THREADS / 32) * MOM_MAXSUMS];
-   const uint32_t cell = blockIdx.x;
-   double* pv = pivot + (size_t)cell * MOM_COUNT;
-   const double U0 = pv[MOM_VX], U1 = pv[MOM_VY], U2 = pv[MOM_VZ];
-   __syncthreads();  // every thread has read U before thread 0 overwrites the record
-   moments_pass<MOM_BOTH>(gids, src_index, data, slots[cell], moments + (size_t)cell * MOM_COUNT, mesh, vmin0, vmin1,
-                          vmin2, bs0, bs1, bs2, dv0, dv1, dv2, mass, charge, U0, U1, U2, sh_hi, sh_lo, pv);
 }
 
 cudaError_t launch_moments_both(const uint32_t* gids, const uint32_t* src_index, const float* data,
                                 const CellSlot* slots, double* pivot, double* moments, const MeshDev& mesh,
                                 const double vmin[3], const double bs[3], const double dv[3], double mass,
-                                double charge, uint32_t n_cells, cudaStream_t stream) {
+                                double charge, uint32_t n_cells, double* part_sums, uint32_t* done, int grid,
+                                cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
-   moments_both_kernel<<<n_cells, MOM_THREADS, 0, stream>>>(gids, src_index, data, slots, pivot, moments, mesh,
-                                                           vmin[0], vmin[1], vmin[2], bs[0], bs[1], bs[2], dv[0],
-                                                           dv[1], dv[2], mass, charge);
+   moments_parts_kernel<MOM_BOTH><<<grid, MOM_THREADS, 0, stream>>>(
+      gids, src_index, data, slots, moments, pivot, nullptr, part_sums, done, mesh, vmin[0], vmin[1], vmin[2], bs[0],
+      bs[1], bs[2], dv[0], dv[1], dv[2], mass, charge, n_cells);
    return cudaGetLastError();
 }
 

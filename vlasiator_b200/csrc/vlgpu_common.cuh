@@ -13,6 +13,11 @@ constexpr int WID3 = 64;
 constexpr int MAX_LEN = 96;         // blocks per mesh axis supported by the 3-word column masks
 constexpr int MAX_PLANE = 96 * 96;  // transverse plane entries
 
+// The moments split a cell's blocks into at most this many parts, each
+// summed by one warp into MOM_SUMS_PER_PART doubles of a work array.
+constexpr int MOM_PARTS_PER_CELL = 64;
+constexpr int MOM_SUMS_PER_PART = 10;
+
 // Per-cell state of one batch, indexed by cell.
 struct CellSlot {
    uint32_t off;     // first block in the current pool
