@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, 3) remap_kernel(
 //    mass of targets above the column's highest cell is moved into it when
 //    the column ends.
 template <int DIM, int RECON>
-__global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 3) remap_walk_kernel(
+__global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) remap_walk_kernel(
    const ColumnSet* __restrict__ sets, SweepCounters* __restrict__ counters, const uint32_t* __restrict__ perm,
    const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
