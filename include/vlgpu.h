@@ -30,6 +30,7 @@ extern "C" {
 #define VLGPU_ECUDA 6     /* CUDA runtime error */
 #define VLGPU_ENODEV 7    /* no CUDA device */
 #define VLGPU_EAGAIN 8    /* a served request has not finished yet */
+#define VLGPU_ENOENT 9    /* no entry (the launch table has none for the device) */
 
 #define VLGPU_CELL_WALL 1u
 #define VLGPU_CELL_RANGE 2u
@@ -345,6 +346,37 @@ int vlgpu_batch_capture(vlgpu_batch* b, int slot, int kind, uint32_t n_steps, co
 /* Launches the graph in `slot` on the batch's stream (asynchronously).
    VLGPU_EINVAL if the batch is not in the buffer state of the capture. */
 int vlgpu_batch_replay(vlgpu_batch* b, int slot);
+
+/* ---- launch shapes and their tuning table (no reference counterpart) ----
+
+   The batch's persistent kernels run with a number of CTAs per SM: the
+   acceleration remap (16 column sets per CTA in flight), the moments, the
+   block adjustment and the translation walk.  0 means the kernel's occupancy
+   maximum (the default); larger values are clamped to it.  Without a
+   vlgpu_batch_set_launch call, every upload consults the tuning table written
+   by vlasiator_b200/autotune.py: per device name and bucket of mean blocks
+   per cell, the fastest shapes of timed steps.  The table is the file
+   $VLGPU_LAUNCH_TABLE, else $XDG_CACHE_HOME/vlgpu/launch_table.tsv (~/.cache
+   when XDG_CACHE_HOME is unset), lines of
+   "<device>\t<lowest mean blocks>\t<remap>\t<moments>\t<adjust>\t<translate>";
+   a missing file or entry means the defaults. */
+typedef struct vlgpu_launch {
+   uint32_t remap_ctas_per_sm;
+   uint32_t moments_ctas_per_sm;
+   uint32_t adjust_ctas_per_sm;
+   uint32_t translate_ctas_per_sm;
+} vlgpu_launch;
+
+/* Sets the shapes (the table is then not consulted); NULL returns the batch
+   to the table at its next upload. */
+int vlgpu_batch_set_launch(vlgpu_batch* b, const vlgpu_launch* cfg);
+
+/* The shapes in use (resolved CTAs per SM; translate 0 = its maximum). */
+int vlgpu_batch_get_launch(vlgpu_batch* b, vlgpu_launch* cfg);
+
+/* The table entry for a device name and mean block count (path NULL: the
+   default table); VLGPU_ENOENT when there is none.  Host only. */
+int vlgpu_launch_table_lookup(const char* path, const char* device, double mean_blocks, vlgpu_launch* out);
 
 /* Synchronises the batch's stream and returns the first error seen. */
 int vlgpu_batch_sync(vlgpu_batch* b);

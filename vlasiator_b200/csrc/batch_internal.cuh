@@ -120,6 +120,12 @@ struct vlgpu_batch {
    cudaStream_t stream = nullptr;
    int sm_count = 0;
    int remap_grid = 0;
+   // launch shapes in CTAs per SM (0 = occupancy maximum): remap, moments,
+   // adjustment, translation; their maxima; whether the caller pinned them
+   uint32_t cps[4] = {0, 0, 0, 0};
+   int cps_max[4] = {0, 0, 0, 0};
+   bool launch_pinned = false;
+   char device_name[256] = {0};  // the key of the launch tuning table
    bool exact = false;  // remap arithmetic: false = fused, true = the reference's operation order
    int recon = 2;       // acceleration reconstruction: 1 PLM, 2 PPM, 4 PQM
    double vmin_d[3], bs_d[3], dv_d[3];
@@ -232,5 +238,7 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool ne
 int translate_device(vlgpu_batch* b, uint32_t dim, double dt);
 int stage_fields(vlgpu_batch* b, const vlgpu_cell_fields* fields, const double* dt);
 int vlasov_step_device(vlgpu_batch* b, double dt, uint32_t map_order);
+void apply_launch(vlgpu_batch* b);
+void consult_launch_table(vlgpu_batch* b, double mean_blocks);
 
 }  // namespace vlgpu_batch_ops

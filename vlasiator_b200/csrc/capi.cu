@@ -257,7 +257,9 @@ int translate_device(vlgpu_batch* b, uint32_t dim, double dt) {
                                 b->grid_dims[2], b->mdev, b->item_gid, b->item_pencil, b->trans_rows,
                                 b->trans_src, b->st_src, (uint32_t)b->capacity, b->row_cap, b->tcounters, b->status,
                                 b->stream));
-   const int grid = b->sm_count * trans_blocks_per_sm(N, b->exact);
+   int per_sm = trans_blocks_per_sm(N, b->exact);
+   if (b->cps[3] > 0 && (int)b->cps[3] < per_sm) per_sm = (int)b->cps[3];
+   const int grid = b->sm_count * per_sm;
    VL_CHECK(launch_trans_remap((int)dim, N, b->item_gid, b->item_pencil, b->trans_rows, b->trans_src, b->tcounters,
                                (uint32_t)b->capacity, b->row_cap, b->st_src, b->data[b->cur], b->data[d], b->gids[d],
                                b->mdev, (float)dt, (float)b->grid_dx[dim], (float)b->params.min_value, b->exact, grid,
@@ -350,9 +352,15 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if (e != cudaSuccess) return fail(e, "cudaSetDevice");
    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
    cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
-   b->remap_grid = b->sm_count * remap_blocks_per_sm();
-   b->adj_grid = b->sm_count * adjust_blocks_per_sm();
-   b->mom_grid = b->sm_count * moments_blocks_per_sm();
+   {
+      cudaDeviceProp prop;
+      if (cudaGetDeviceProperties(&prop, device) == cudaSuccess)
+         std::snprintf(b->device_name, sizeof b->device_name, "%s", prop.name);
+   }
+   b->cps_max[0] = remap_blocks_per_sm();
+   b->cps_max[1] = moments_blocks_per_sm();
+   b->cps_max[2] = adjust_blocks_per_sm();
+   apply_launch(b);
    const uint64_t cap = block_capacity;
    for (int p = 0; p < 2; ++p) {
       if ((e = cudaMalloc(&b->gids[p], sizeof(uint32_t) * cap)) != cudaSuccess) return fail(e, "gids");
@@ -449,6 +457,7 @@ int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* 
    }
    set_direct_state(b, 0);
    b->content_valid = false;
+   consult_launch_table(b, (double)total / b->n_cells);
    return VLGPU_OK;
 }
 
@@ -478,6 +487,7 @@ int vlgpu_batch_upload_async(vlgpu_batch* b, const uint64_t* offsets, const uint
    VL_CHECK(cudaEventRecord(b->ev_upload, b->stream));
    set_direct_state(b, 0);
    b->content_valid = false;
+   consult_launch_table(b, (double)hs[b->n_cells].off / b->n_cells);
    return VLGPU_OK;
 }
 

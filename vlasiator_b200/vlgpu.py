@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvlgpu.so")
 
 STATUS = {0: "VLGPU_OK", 1: "VLGPU_EINVAL", 2: "VLGPU_ENOMEM", 3: "VLGPU_EWALL", 4: "VLGPU_ETIMEDOUT",
-          5: "VLGPU_ERANGE", 6: "VLGPU_ECUDA", 7: "VLGPU_ENODEV", 8: "VLGPU_EAGAIN"}
+          5: "VLGPU_ERANGE", 6: "VLGPU_ECUDA", 7: "VLGPU_ENODEV", 8: "VLGPU_EAGAIN", 9: "VLGPU_ENOENT"}
 CELL_WALL, CELL_RANGE, CELL_NOMEM, CELL_BADDK = 1, 2, 4, 8
 
 
@@ -57,6 +57,16 @@ class CFieldsT(ctypes.Structure):
 _lib = None
 
 # every symbol include/vlgpu.h declares, with its ctypes signature
+class CLaunchT(ctypes.Structure):
+    """vlgpu_launch: CTAs per SM of the remap, moments, adjustment and translation kernels (0 = maximum)."""
+    _fields_ = [("remap_ctas_per_sm", ctypes.c_uint32), ("moments_ctas_per_sm", ctypes.c_uint32),
+                ("adjust_ctas_per_sm", ctypes.c_uint32), ("translate_ctas_per_sm", ctypes.c_uint32)]
+
+    def as_tuple(self):
+        return (self.remap_ctas_per_sm, self.moments_ctas_per_sm, self.adjust_ctas_per_sm,
+                self.translate_ctas_per_sm)
+
+
 _vp = ctypes.c_void_p
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -114,6 +124,10 @@ SIGNATURES = {
     "vlgpu_map_1d_noalloc": (ctypes.c_int, [ctypes.POINTER(CMeshT), ctypes.POINTER(CParamsT), ctypes.c_uint32, _u64p,
                                             _vp, _vp, _dp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _u32p, _u32p,
                                             _u32p, _vp]),
+    "vlgpu_batch_set_launch": (ctypes.c_int, [_vp, ctypes.POINTER(CLaunchT)]),
+    "vlgpu_batch_get_launch": (ctypes.c_int, [_vp, ctypes.POINTER(CLaunchT)]),
+    "vlgpu_launch_table_lookup": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                                 ctypes.POINTER(CLaunchT)]),
     "vlgpu_version": (ctypes.c_char_p, []),
 }
 
@@ -413,6 +427,21 @@ class Batch:
         out = np.zeros((self.n_cells, 12))
         _check(self.lib.vlgpu_batch_intersections(self.h, _p(out, ctypes.c_double)), "vlgpu_batch_intersections")
         return out
+
+    def set_launch(self, shapes=None):
+        """CTAs per SM of the remap, moments, adjustment and translation kernels
+        (a 4-tuple, 0 = the occupancy maximum); None: the tuning table again."""
+        if shapes is None:
+            _check(self.lib.vlgpu_batch_set_launch(self.h, None), "vlgpu_batch_set_launch")
+            return
+        cfg = CLaunchT(*[int(x) for x in shapes])
+        _check(self.lib.vlgpu_batch_set_launch(self.h, ctypes.byref(cfg)), "vlgpu_batch_set_launch")
+
+    def launch(self):
+        """The launch shapes in use, resolved to CTAs per SM (translate 0 = its maximum)."""
+        cfg = CLaunchT()
+        _check(self.lib.vlgpu_batch_get_launch(self.h, ctypes.byref(cfg)), "vlgpu_batch_get_launch")
+        return cfg.as_tuple()
 
     def stream_handle(self) -> int:
         s = _vp()
