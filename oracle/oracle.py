@@ -294,7 +294,7 @@ class ReferenceBuild:
                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32, ctypes.c_int, _dp]
         L.ref_cells_vlasov_step.argtypes = [_vp, _u32p, _dp, _dp, ctypes.c_double, ctypes.c_uint32, ctypes.c_double,
                                             ctypes.c_double, ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32,
-                                            ctypes.c_int]
+                                            ctypes.c_int, _dp, _dp]
         L.ref_map_order.restype = ctypes.c_uint32
         L.ref_map_order.argtypes = [ctypes.c_uint32]
         L.ref_cells_content.restype = ctypes.c_uint64
@@ -396,16 +396,22 @@ class ReferenceBuild:
                                      mass, nb, k, nthreads, None if out is None else _ptr(out, ctypes.c_double))
         return out
 
-    def vlasov_step(self, h, grid, dx, B, dt, map_order, charge, mass, neighbors, nthreads=0):
+    def vlasov_step(self, h, grid, dx, B, dt, map_order, charge, mass, neighbors, nthreads=0, moments=False):
         """One full Vlasov step of the periodic grid: translation z, x, y, the _R
-        moments, then full_step with the spatial neighbours."""
+        moments, then full_step with the spatial neighbours.  With moments=True
+        returns ((n_cells, 10) moments as full_step, the RHOLOSSADJUST each cell
+        gained in the step)."""
         g = np.ascontiguousarray(grid, np.uint32)
         d = np.ascontiguousarray(np.broadcast_to(np.asarray(dx, np.float64), (3,)))
         B = np.ascontiguousarray(B, np.float64)
         nb, k = self._neighbors(neighbors)
+        out = np.zeros((len(B), 10)) if moments else None
+        loss = np.zeros(len(B)) if moments else None
         self.lib.ref_cells_vlasov_step(h, _ptr(g, ctypes.c_uint32), _ptr(d, ctypes.c_double),
                                        _ptr(B, ctypes.c_double), float(dt), map_order, charge, mass, nb, k,
-                                       nthreads)
+                                       nthreads, None if out is None else _ptr(out, ctypes.c_double),
+                                       None if loss is None else _ptr(loss, ctypes.c_double))
+        return (out, loss) if moments else None
 
     def _neighbors(self, neighbors):
         if neighbors is None:

@@ -369,15 +369,19 @@ void ref_cells_translate(void* h, const uint32_t grid[3], uint32_t dimension, do
 // reference's main-loop order: calculateSpatialTranslation (trans_map_1d_amr
 // along z, x, y, vlasovmover.cpp:65-381) and the "_R" moments, then the full
 // acceleration step above with the spatial neighbours in the adjustment.
+// moments_out (n_cells x 10, as ref_cells_full_step) and rho_loss (the
+// RHOLOSSADJUST each cell gained in the step) may be null.
 void ref_cells_vlasov_step(void* h, const uint32_t grid[3], const double dx[3], const double* B, double dt,
                            uint32_t map_order, double charge, double mass, const int32_t* neighbors,
-                           uint32_t n_per_cell, int nthreads) {
+                           uint32_t n_per_cell, int nthreads, double* moments_out, double* rho_loss) {
    RefCells* rc = (RefCells*)h;
    static const uint32_t dims[3] = {2, 0, 1};
    for (uint32_t q = 0; q < 3; ++q) ref_cells_translate(h, grid, dims[q], dt, dx[dims[q]], nthreads);
    moments_cells(rc, nullptr);
    std::vector<double> dts(rc->cells.size(), dt);
-   ref_cells_full_step(h, B, dts.data(), map_order, charge, mass, neighbors, n_per_cell, nthreads, nullptr);
+   ref_cells_accelerate_step(h, B, dts.data(), map_order, charge, mass, nthreads);
+   adjust_cells(rc, neighbors, n_per_cell, rho_loss);
+   moments_cells(rc, moments_out);
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }

@@ -61,9 +61,11 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
-                          uint32_t n_cells, uint32_t* scratch, int grid, MaskRec* masks, uint32_t* pool,
-                          uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream);
+                          uint32_t n_cells, uint32_t* scratch, int grid, int wide_grid, uint32_t* wide_cells,
+                          MaskRec* masks, uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap,
+                          cudaStream_t stream);
 int adjust_blocks_per_sm();
+int adjust_warp_blocks_per_sm();
 size_t adjust_scratch_words(const MeshDev& mesh);
 cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const CellAccelInputs* in, const MeshDev& mesh,
                           const double vmin[3], const double bs[3], const double dv[3], const double dx[3], double q,
@@ -178,12 +180,14 @@ struct vlgpu_batch {
    TransCounters* tcounters = nullptr;
    int32_t* neighbors = nullptr;  // 26 per cell (-1: none), the spatial neighbours block adjustment consults
    double* dt_buf = nullptr;      // 2 per cell: r-space and v-space time-step limits
-   uint32_t* adj_scratch = nullptr;  // per adjustment CTA: masks of a cell too wide for shared memory
+   uint32_t* adj_scratch = nullptr;  // per CTA of the wide-cell adjustment: masks too wide for shared memory
+   uint32_t* adj_wide_cells = nullptr;  // the cells the warp-per-cell adjustment leaves to the wide-cell one
    vlgpu::MaskRec* mask_recs = nullptr;  // grid: per cell, its content mask record
    uint32_t* mask_pool = nullptr;        // grid: the content mask rows
    uint32_t* mask_top = nullptr;         // grid: words of the pool in use
    uint32_t mask_cap = 0;
-   int adj_grid = 0;
+   int adj_grid = 0;       // CTAs of the warp-per-cell adjustment
+   int adj_wide_grid = 0;  // CTAs of the wide-cell adjustment
    double* moments_r = nullptr;   // MOM_COUNT per cell: the moments after translation (the "_R" set)
    // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;

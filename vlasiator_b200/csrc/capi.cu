@@ -48,6 +48,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
    cudaFree(b->adj_scratch);
+   cudaFree(b->adj_wide_cells);
    cudaFree(b->mask_recs);
    cudaFree(b->mask_pool);
    cudaFree(b->mask_top);
@@ -161,8 +162,9 @@ int adjust_device(vlgpu_batch* b) {
                           b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
                           (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid,
-                          b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, b->stream));
-   b->launches += (b->neighbors && b->mask_recs) ? 2 : 1;  // content masks first on a grid
+                          b->adj_wide_grid, b->adj_wide_cells, b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap,
+                          b->stream));
+   b->launches += (b->neighbors && b->mask_recs) ? 3 : 2;  // content masks first on a grid
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
    b->st_gids = b->adj_gids[a];
@@ -359,7 +361,8 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    }
    b->cps_max[0] = remap_blocks_per_sm();
    b->cps_max[1] = moments_blocks_per_sm();
-   b->cps_max[2] = adjust_blocks_per_sm();
+   b->cps_max[2] = adjust_warp_blocks_per_sm();
+   b->adj_wide_grid = b->sm_count * adjust_blocks_per_sm();
    apply_launch(b);
    const uint64_t cap = block_capacity;
    for (int p = 0; p < 2; ++p) {
@@ -399,9 +402,10 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMalloc(&b->stats, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMalloc(&b->rows_used, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMalloc(&b->adj_scratch, sizeof(uint32_t) * adjust_scratch_words(b->mdev) *
-                                            (size_t)std::min<uint32_t>((uint32_t)b->adj_grid, n_cells))) !=
+                                            (size_t)std::min<uint32_t>((uint32_t)b->adj_wide_grid, n_cells))) !=
        cudaSuccess)
       return fail(e, "adjust scratch");
+   if ((e = cudaMalloc(&b->adj_wide_cells, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "adjust");
    if ((e = cudaMemset(b->rows_used, 0, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMemset(b->stats, 0, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMallocHost(&b->h_sweep, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "pinned");
