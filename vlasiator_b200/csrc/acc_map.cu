@@ -186,21 +186,20 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
    return before + x - v;
 }
 
+// The column structure of one cell, by the whole CTA (see the file header).
 template <int DIM>
-__global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
-   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ src_slots,
-   CellSlot* __restrict__ dst_slots, uint32_t* __restrict__ perm, ColumnSet* __restrict__ sets,
-   uint32_t set_capacity, uint32_t dst_capacity,
+__device__ __forceinline__ void columnize_cell(
+   uint32_t cell, const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index,
+   const CellSlot* __restrict__ src_slots, CellSlot* __restrict__ dst_slots, uint32_t* __restrict__ perm,
+   ColumnSet* __restrict__ sets, uint32_t set_capacity, uint32_t dst_capacity,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
-   BatchStats* __restrict__ stats, MeshDev mesh, int wall_margin, uint32_t cell_begin, uint32_t cell_end,
-   int first_of_step) {
+   BatchStats* __restrict__ stats, const MeshDev& mesh, int wall_margin, int first_of_step, uint32_t plane_cap,
+   uint32_t* __restrict__ wide_cells) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
    __shared__ uint32_t s_bbox[4];
    __shared__ uint32_t s_set_base, s_dst_base, s_nsets, s_ntgt, s_flags;
 
-   const uint32_t cell = cell_begin + blockIdx.x;
-   if (cell >= cell_end) return;
    const CellSlot src = src_slots[cell];
    const SweepCell P = sweep_cells[cell];
    uint32_t li, lj;
@@ -216,7 +215,10 @@ __global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
       if (threadIdx.x == 0) dst_slots[cell] = CellSlot{0u, 0u};
       return;
    }
-   // pass 1: bounding box of the transverse indices
+   constexpr uint32_t FULL = 0xffffffffu;
+   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   // pass 1: bounding box of the transverse indices (warp reductions, one
+   // shared min/max per warp)
    {
       uint32_t a0 = 0xffffffffu, a1 = 0, b0 = 0xffffffffu, b1 = 0;
       for (uint32_t b = threadIdx.x; b < src.count; b += blockDim.x) {
@@ -225,25 +227,49 @@ __global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
          a0 = min(a0, s[0]); a1 = max(a1, s[0]);
          b0 = min(b0, s[1]); b1 = max(b1, s[1]);
       }
-      atomicMin(&s_bbox[0], a0); atomicMax(&s_bbox[1], a1);
-      atomicMin(&s_bbox[2], b0); atomicMax(&s_bbox[3], b1);
+      a0 = __reduce_min_sync(FULL, a0); a1 = __reduce_max_sync(FULL, a1);
+      b0 = __reduce_min_sync(FULL, b0); b1 = __reduce_max_sync(FULL, b1);
+      if (lane == 0) {
+         atomicMin(&s_bbox[0], a0); atomicMax(&s_bbox[1], a1);
+         atomicMin(&s_bbox[2], b0); atomicMax(&s_bbox[3], b1);
+      }
    }
    __syncthreads();
    const uint32_t a_lo = s_bbox[0], b_lo = s_bbox[2];
    const uint32_t na = s_bbox[1] - a_lo + 1, nb = s_bbox[3] - b_lo + 1;
    const uint32_t plane = na * nb;
+   if (plane > plane_cap) {
+      // too wide for this launch's shared memory: left to columnize_wide_kernel
+      if (threadIdx.x == 0) wide_cells[atomicAdd(&counters->n_wide, 1u)] = cell;
+      return;
+   }
    uint32_t* mask = smem;                   // 3 * plane
    uint32_t* prefix = smem + 3 * plane;     // plane
    uint16_t* set_t = (uint16_t*)(prefix + plane);  // plane (set index -> t)
    uint32_t* tcount = prefix + plane + (plane + 1) / 2;  // plane
    for (uint32_t q = threadIdx.x; q < 3 * plane; q += blockDim.x) mask[q] = 0;
    __syncthreads();
-   // pass 2: occupancy masks along the sweep dimension
-   for (uint32_t b = threadIdx.x; b < src.count; b += blockDim.x) {
-      uint32_t s[3];
-      swapped_indices(gids[src.off + b], mesh.len, DIM, s);
-      const uint32_t t = (s[0] - a_lo) * nb + (s[1] - b_lo);
-      atomicOr(&mask[3 * t + (s[2] >> 5)], 1u << (s[2] & 31));
+   // pass 2: occupancy masks along the sweep dimension; lanes that set bits
+   // of one word (a run of the list along the sweep) combine them first
+   for (uint32_t b0 = warp * 32; b0 < src.count; b0 += blockDim.x) {
+      const uint32_t b = b0 + lane;
+      uint32_t key = 0xffffffffu, bit = 0u;
+      if (b < src.count) {
+         uint32_t s[3];
+         swapped_indices(gids[src.off + b], mesh.len, DIM, s);
+         key = 3 * ((s[0] - a_lo) * nb + (s[1] - b_lo)) + (s[2] >> 5);
+         bit = 1u << (s[2] & 31);
+      }
+      const uint32_t match = __match_any_sync(FULL, key);
+      const bool big = key != 0xffffffffu && __popc(match) >= 4;
+      if (key != 0xffffffffu && !big) atomicOr(&mask[key], bit);
+      for (uint32_t leaders = __ballot_sync(FULL, big && (int)lane == __ffs(match) - 1); leaders;
+           leaders &= leaders - 1) {
+         const int leader = __ffs(leaders) - 1;
+         const bool mine = (__shfl_sync(FULL, match, leader) >> lane) & 1u;
+         const uint32_t bits = __reduce_or_sync(FULL, mine ? bit : 0u);
+         if ((int)lane == leader) atomicOr(&mask[key], bits);
+      }
    }
    __syncthreads();
    // scan over the plane: source offsets and set indices
@@ -360,6 +386,41 @@ __global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
       dst_slots[cell] = ok ? CellSlot{s_dst_base, s_ntgt} : CellSlot{0u, 0u};
       if (s_flags) atomicOr(&status[cell], s_flags);
       if (!ok) atomicOr(&counters->overflow, 1u);
+   }
+}
+
+// One CTA per cell of [cell_begin, cell_end).
+template <int DIM>
+__global__ void __launch_bounds__(COL_THREADS) columnize_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ src_slots,
+   CellSlot* __restrict__ dst_slots, uint32_t* __restrict__ perm, ColumnSet* __restrict__ sets,
+   uint32_t set_capacity, uint32_t dst_capacity,
+   const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
+   BatchStats* __restrict__ stats, MeshDev mesh, int wall_margin, uint32_t cell_begin, uint32_t cell_end,
+   int first_of_step, const uint32_t* __restrict__ order, uint32_t plane_cap, uint32_t* __restrict__ wide_cells) {
+   if (cell_begin + blockIdx.x >= cell_end) return;
+   const uint32_t cell = order ? order[blockIdx.x] : cell_begin + blockIdx.x;
+   columnize_cell<DIM>(cell, gids, src_index, src_slots, dst_slots, perm, sets, set_capacity, dst_capacity,
+                       sweep_cells, status, counters, stats, mesh, wall_margin, first_of_step, plane_cap,
+                       wide_cells);
+}
+
+// Persistent CTAs over the cells whose plane did not fit the capped launch
+// (wide_cells, counters->n_wide of them), with a full plane of shared memory.
+template <int DIM>
+__global__ void __launch_bounds__(COL_THREADS) columnize_wide_kernel(
+   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ src_slots,
+   CellSlot* __restrict__ dst_slots, uint32_t* __restrict__ perm, ColumnSet* __restrict__ sets,
+   uint32_t set_capacity, uint32_t dst_capacity,
+   const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
+   BatchStats* __restrict__ stats, MeshDev mesh, int wall_margin, int first_of_step,
+   const uint32_t* __restrict__ wide_cells) {
+   const uint32_t n = counters->n_wide;
+   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
+      columnize_cell<DIM>(wide_cells[it], gids, src_index, src_slots, dst_slots, perm, sets, set_capacity,
+                          dst_capacity, sweep_cells, status, counters, stats, mesh, wall_margin, first_of_step,
+                          0xffffffffu, nullptr);
+      __syncthreads();  // the next cell reuses the shared state
    }
 }
 
@@ -956,10 +1017,63 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
    columnize_kernel<D><<<n, COL_THREADS, smem, stream>>>(gids, src_index, src_slots, dst_slots, perm, sets,      \
                                                          set_capacity,                                          \
                                                          dst_capacity, sweep_cells, status, counters, stats, mesh, \
-                                                         wall_margin, cell_begin, cell_end, first_of_step);
+                                                         wall_margin, cell_begin, cell_end, first_of_step, nullptr, \
+                                                         0xffffffffu, nullptr);
    if (dim == 0) { VLGPU_COL(0) } else if (dim == 1) { VLGPU_COL(1) } else { VLGPU_COL(2) }
 #undef VLGPU_COL
    return cudaGetLastError();
+}
+
+// Columnize of every cell of a batch: one CTA per cell, the largest cells
+// first (order), with shared memory for planes of up to COL_CAP_PLANE entries,
+// which lets four CTAs share an SM; the cells with wider planes follow in
+// columnize_wide_kernel.  The counters' n_wide must be zero (the caller clears
+// the sweep counters before every sweep).
+constexpr uint32_t COL_CAP_PLANE = 1024;
+cudaError_t launch_columnize_batch(int dim, const uint32_t* gids, const uint32_t* src_index,
+                                   const CellSlot* src_slots, CellSlot* dst_slots, uint32_t* perm, ColumnSet* sets,
+                                   uint32_t set_capacity, uint32_t dst_capacity, const SweepCell* sweep_cells,
+                                   uint32_t* status, SweepCounters* counters, BatchStats* stats, const MeshDev& mesh,
+                                   int wall_margin, uint32_t n_cells, int first_of_step, uint32_t* wide_cells,
+                                   const uint32_t* order, int wide_grid, cudaStream_t stream) {
+   if (n_cells == 0) return cudaSuccess;
+   uint32_t li, lj;
+   plane_lengths(mesh.len, dim, li, lj);
+   const uint32_t cap = li * lj < COL_CAP_PLANE ? li * lj : COL_CAP_PLANE;
+   const size_t smem_cap = columnize_smem_bytes(cap);
+   const size_t smem = columnize_smem_bytes(li * lj);
+   const uint32_t g2 = (uint32_t)wide_grid < n_cells ? (uint32_t)wide_grid : n_cells;
+   cudaError_t e = cudaSuccess;
+#define VLGPU_COLB(D)                                                                                           \
+   e = cudaFuncSetAttribute(columnize_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+   if (e != cudaSuccess) return e;                                                                               \
+   e = cudaFuncSetAttribute(columnize_wide_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+   if (e != cudaSuccess) return e;                                                                               \
+   columnize_kernel<D><<<n_cells, COL_THREADS, smem_cap, stream>>>(                                              \
+      gids, src_index, src_slots, dst_slots, perm, sets, set_capacity, dst_capacity, sweep_cells, status, counters, \
+      stats, mesh, wall_margin, 0, n_cells, first_of_step, order, cap, wide_cells);                              \
+   columnize_wide_kernel<D><<<g2, COL_THREADS, smem, stream>>>(gids, src_index, src_slots, dst_slots, perm, sets, \
+                                                               set_capacity, dst_capacity, sweep_cells, status,   \
+                                                               counters, stats, mesh, wall_margin, first_of_step, \
+                                                               wide_cells);
+   if (dim == 0) { VLGPU_COLB(0) } else if (dim == 1) { VLGPU_COLB(1) } else { VLGPU_COLB(2) }
+#undef VLGPU_COLB
+   return cudaGetLastError();
+}
+
+// CTAs per SM of columnize_wide_kernel (the largest plane of the three
+// dimensions).
+int columnize_wide_blocks_per_sm(const MeshDev& mesh) {
+   uint32_t li, lj, best = 0;
+   for (int d = 0; d < 3; ++d) {
+      plane_lengths(mesh.len, d, li, lj);
+      best = li * lj > best ? li * lj : best;
+   }
+   const size_t smem = columnize_smem_bytes(best);
+   int n = 0;
+   cudaFuncSetAttribute(columnize_wide_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, columnize_wide_kernel<0>, COL_THREADS, smem);
+   return n > 0 ? n : 1;
 }
 
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,

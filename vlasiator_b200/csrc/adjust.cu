@@ -11,8 +11,9 @@
 // in H are removed and their mass sum(f)*dv^3 is added to RHOLOSSADJUST,
 // blocks of H that did not exist are added with zero data.
 //
-// One CTA per cell.  The content set and H live in shared memory as 96-bit
-// x-masks over the (y,z) rows of the cell's dilated bounding box.  The output
+// Persistent CTAs of 256 threads, one cell at a time, the largest cells
+// first.  The content set and H live in shared memory as 96-bit x-masks over
+// the (y,z) rows of the cell's dilated bounding box.  The output
 // is a new block list sorted by global ID plus, per block, the index of its
 // data in the current pool (or none for an added block): no VDF value is
 // copied, the next sweep reads the kept blocks where they are.
@@ -28,7 +29,9 @@
 
 namespace vlgpu {
 
-constexpr int ADJ_THREADS = 512;
+constexpr int ADJ_THREADS = 256;
+constexpr int ADJ_MIN_CTAS = 4;   // CTAs per SM the register budget is set for
+constexpr int ADJ_UNROLL = 2;     // list entries per thread in flight
 constexpr uint32_t NO_BLOCK = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t adj_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
@@ -165,36 +168,51 @@ __global__ void __launch_bounds__(MASK_THREADS) content_mask_kernel(
       for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) pool[off + q] = C[q];
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
+// One cell at a time per CTA of ADJ_THREADS threads; persistent CTAs take
+// the cells from a counter in the order `order` gives (largest first), so
+// the longest cells start first and the rest balance over the CTAs.  Per
+// cell: the content bounding box, the content mask C (one shared-memory OR
+// per content block, after the lanes of a warp that set bits of the same
+// word combine them), the dilated set H row by row, the neighbours' content,
+// an exclusive scan of the row counts, the GID-sorted output list, and a pass
+// over the old blocks that points kept entries at their data and sums the
+// removed ones (a half-warp per removed block, float4 rows).
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
    const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
    const uint8_t* __restrict__ content, const float* __restrict__ data, const int32_t* __restrict__ neighbors,
    uint32_t* __restrict__ out_gids, uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots,
    double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
    uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3, uint32_t n_cells,
    uint32_t smem_rows, uint32_t* __restrict__ scratch, const MaskRec* __restrict__ masks,
-   const uint32_t* __restrict__ pool, const uint32_t* __restrict__ cell_list) {
+   const uint32_t* __restrict__ pool, const uint32_t* __restrict__ order) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
    __shared__ int s_box[8];
-   __shared__ uint32_t s_base, s_flags;
+   __shared__ uint32_t s_base, s_flags, s_item;
    __shared__ double s_loss[ADJ_THREADS / 32];
-   __shared__ MaskRec s_rec[27];  // the neighbours' content masks (26: the cell's own)
+   __shared__ MaskRec s_rec[27];     // the neighbours' content masks (26: the cell's own)
    __shared__ uint32_t s_first[27];  // first mask-row item of each neighbour
-
-   // persistent CTAs, one cell at a time: every cell, or the cells that
-   // adjust_warp_kernel left (cell_list, counters->adj_wide of them)
-   const uint32_t n_items = cell_list ? counters->adj_wide : n_cells;
-   for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-   const uint32_t cell = cell_list ? cell_list[item] : item;
-   const CellSlot s = slots[cell];
+   constexpr uint32_t FULL = 0xffffffffu;
+   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    const uint32_t L0 = mesh.len[0], L1 = mesh.len[1], L2 = mesh.len[2];
+   const uint32_t xmask2 = (L0 >= 96) ? 0xffffffffu : ((L0 <= 64) ? 0u : ((1u << (L0 - 64)) - 1u));
+   const uint32_t xmask1 = (L0 >= 64) ? 0xffffffffu : ((L0 <= 32) ? 0u : ((1u << (L0 - 32)) - 1u));
+   const uint32_t xmask0 = (L0 >= 32) ? 0xffffffffu : ((1u << L0) - 1u);
+
+   for (;;) {
    if (threadIdx.x == 0) {
+      s_item = atomicAdd(&counters->cell_next, 1u);
       for (int q = 0; q < 8; q += 2) {
          s_box[q] = 1 << 20;
          s_box[q + 1] = -1;
       }
       s_flags = 0;
    }
+   __syncthreads();
+   const uint32_t item = s_item;
+   if (item >= n_cells) break;
+   const uint32_t cell = order[item];
+   const CellSlot s = slots[cell];
    if (threadIdx.x < 27) {
       // mask records of the neighbours (a missing neighbour reads as empty)
       // and of the cell itself; without masks every list is walked
@@ -208,7 +226,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    }
    __syncthreads();
    // pass 1: bounding boxes (y, z) of the cell's content blocks and of its
-   // spatial neighbours' content blocks
+   // spatial neighbours' content blocks (warp reductions, one shared
+   // min/max per warp)
    {
       const bool own_mask = s_rec[26].off != NO_MASK;
       if (own_mask) {
@@ -218,17 +237,30 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
          }
       } else {
          int y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
-         for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-            if (list_block_content(src_index, content, data, s.off + b, min_value)) {
-               const uint32_t g = gids[s.off + b];
+         for (uint32_t b0 = threadIdx.x; b0 < s.count; b0 += ADJ_THREADS * ADJ_UNROLL) {
+            bool c[ADJ_UNROLL];
+            uint32_t g[ADJ_UNROLL];
+#pragma unroll
+            for (int u = 0; u < ADJ_UNROLL; ++u) {
+               const uint32_t b = b0 + ADJ_THREADS * u;
+               c[u] = b < s.count && list_block_content(src_index, content, data, s.off + b, min_value);
+               g[u] = b < s.count ? gids[s.off + b] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < ADJ_UNROLL; ++u) {
+               if (!c[u]) continue;
                uint32_t bx, by, bz;
-            block_xyz(mesh, g, bx, by, bz);
-            const int y = (int)by, z = (int)bz;
-               y0 = min(y0, y); y1 = max(y1, y); z0 = min(z0, z); z1 = max(z1, z);
+               block_xyz(mesh, g[u], bx, by, bz);
+               y0 = min(y0, (int)by); y1 = max(y1, (int)by);
+               z0 = min(z0, (int)bz); z1 = max(z1, (int)bz);
             }
          }
-         atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
-         atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
+         y0 = __reduce_min_sync(FULL, y0); y1 = __reduce_max_sync(FULL, y1);
+         z0 = __reduce_min_sync(FULL, z0); z1 = __reduce_max_sync(FULL, z1);
+         if (lane == 0) {
+            atomicMin(&s_box[0], y0); atomicMax(&s_box[1], y1);
+            atomicMin(&s_box[2], z0); atomicMax(&s_box[3], z1);
+         }
       }
       if (neighbors) {
          int ny0 = 1 << 20, ny1 = -1, nz0 = 1 << 20, nz1 = -1;
@@ -240,18 +272,21 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
             const int32_t nc = neighbors[(size_t)cell * 26 + q];
             if (nc < 0 || s_rec[q].off != NO_MASK) continue;
             const CellSlot ns = slots[nc];
-            for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
+            for (uint32_t b = threadIdx.x; b < ns.count; b += ADJ_THREADS) {
                if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
-                  const uint32_t g = gids[ns.off + b];
                   uint32_t bx, by, bz;
-            block_xyz(mesh, g, bx, by, bz);
-            const int y = (int)by, z = (int)bz;
-                  ny0 = min(ny0, y); ny1 = max(ny1, y); nz0 = min(nz0, z); nz1 = max(nz1, z);
+                  block_xyz(mesh, gids[ns.off + b], bx, by, bz);
+                  ny0 = min(ny0, (int)by); ny1 = max(ny1, (int)by);
+                  nz0 = min(nz0, (int)bz); nz1 = max(nz1, (int)bz);
                }
             }
          }
-         atomicMin(&s_box[4], ny0); atomicMax(&s_box[5], ny1);
-         atomicMin(&s_box[6], nz0); atomicMax(&s_box[7], nz1);
+         ny0 = __reduce_min_sync(FULL, ny0); ny1 = __reduce_max_sync(FULL, ny1);
+         nz0 = __reduce_min_sync(FULL, nz0); nz1 = __reduce_max_sync(FULL, nz1);
+         if (lane == 0) {
+            atomicMin(&s_box[4], ny0); atomicMax(&s_box[5], ny1);
+            atomicMin(&s_box[6], nz0); atomicMax(&s_box[7], nz1);
+         }
       }
    }
    __syncthreads();
@@ -275,7 +310,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    uint32_t* C = base;              // 3 * rows
    uint32_t* H = base + 3 * rows;   // 3 * rows
    uint32_t* prefix = base + 6 * rows;  // rows
-   for (uint32_t q = threadIdx.x; q < 3 * rows; q += blockDim.x) C[q] = 0;
+   for (uint32_t q = threadIdx.x; q < 3 * rows; q += ADJ_THREADS) C[q] = 0;
    __syncthreads();
    // pass 2: content mask rows (copied from the cell's own mask when it has one)
    if (s_rec[26].off != NO_MASK) {
@@ -283,30 +318,49 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       if (m.y1 >= 0) {
          const int my = m.y1 - m.y0 + 1;
          const uint32_t mrows = (uint32_t)(my * (m.z1 - m.z0 + 1));
-         for (uint32_t q = threadIdx.x; q < 3 * mrows; q += blockDim.x) {
+         for (uint32_t q = threadIdx.x; q < 3 * mrows; q += ADJ_THREADS) {
             const uint32_t mr = q / 3, w = q - 3 * mr;
             const int y = m.y0 + (int)(mr % my), z = m.z0 + (int)(mr / my);
             C[3 * (uint32_t)((z - z0) * ny + (y - y0)) + w] = pool[m.off + q];
          }
       }
-   } else {
-      for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-         if (list_block_content(src_index, content, data, s.off + b, min_value)) {
-            const uint32_t g = gids[s.off + b];
-            uint32_t x, by, bz;
-            block_xyz(mesh, g, x, by, bz);
-            const int y = (int)by, z = (int)bz;
-            const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
-            atomicOr(&C[3 * r + (x >> 5)], 1u << (x & 31));
+   } else if (own_any) {
+      for (uint32_t b0 = warp * 32; b0 < s.count; b0 += ADJ_THREADS * ADJ_UNROLL) {
+         bool cc[ADJ_UNROLL];
+         uint32_t gg[ADJ_UNROLL];
+#pragma unroll
+         for (int u = 0; u < ADJ_UNROLL; ++u) {
+            const uint32_t b = b0 + ADJ_THREADS * u + lane;
+            cc[u] = b < s.count && list_block_content(src_index, content, data, s.off + b, min_value);
+            gg[u] = b < s.count ? gids[s.off + b] : 0u;
+         }
+#pragma unroll
+         for (int u = 0; u < ADJ_UNROLL; ++u) {
+            uint32_t key = 0xffffffffu, bit = 0u;
+            if (cc[u]) {
+               uint32_t x, by, bz;
+               block_xyz(mesh, gg[u], x, by, bz);
+               key = 3 * (uint32_t)(((int)bz - z0) * ny + ((int)by - y0)) + (x >> 5);
+               bit = 1u << (x & 31);
+            }
+            // lanes that set bits of one word (a run of the list along x):
+            // four or more combine them first
+            const uint32_t match = __match_any_sync(FULL, key);
+            const bool big = cc[u] && __popc(match) >= 4;
+            if (cc[u] && !big) atomicOr(&C[key], bit);
+            for (uint32_t leaders = __ballot_sync(FULL, big && (int)lane == __ffs(match) - 1); leaders;
+                 leaders &= leaders - 1) {
+               const int leader = __ffs(leaders) - 1;
+               const bool mine = (__shfl_sync(FULL, match, leader) >> lane) & 1u;
+               const uint32_t bits = __reduce_or_sync(FULL, mine ? bit : 0u);
+               if ((int)lane == leader) atomicOr(&C[key], bits);
+            }
          }
       }
    }
    __syncthreads();
    // dilation: H(y,z) = OR over |dy|,|dz| <= w of the row dilated along x
-   const uint32_t xmask2 = (L0 >= 96) ? 0xffffffffu : ((L0 <= 64) ? 0u : ((1u << (L0 - 64)) - 1u));
-   const uint32_t xmask1 = (L0 >= 64) ? 0xffffffffu : ((L0 <= 32) ? 0u : ((1u << (L0 - 32)) - 1u));
-   const uint32_t xmask0 = (L0 >= 32) ? 0xffffffffu : ((1u << L0) - 1u);
-   const uint32_t chunk = (rows + blockDim.x - 1) / blockDim.x;
+   const uint32_t chunk = (rows + ADJ_THREADS - 1) / ADJ_THREADS;
    const uint32_t r0 = min(rows, threadIdx.x * chunk), r1 = min(rows, r0 + chunk);
    for (uint32_t r = r0; r < r1; ++r) {
       const int yy = y0 + (int)(r % ny), zz = z0 + (int)(r / ny);
@@ -349,7 +403,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
          __syncthreads();
          const uint32_t items = s_first[26];
          int q = 0;
-         for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
+         for (uint32_t it = threadIdx.x; it < items; it += ADJ_THREADS) {
             while (it >= s_first[q + 1]) ++q;
             const MaskRec& m = s_rec[q];
             const uint32_t mr = it - s_first[q];
@@ -363,19 +417,16 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
             if (w1) atomicOr(dst + 1, w1);
             if (w2) atomicOr(dst + 2, w2);
          }
-         __syncthreads();
       }
       for (int q = 0; q < 26; ++q) {
          const int32_t nc = neighbors[(size_t)cell * 26 + q];
          if (nc < 0 || s_rec[q].off != NO_MASK) continue;
          const CellSlot ns = slots[nc];
-         for (uint32_t b = threadIdx.x; b < ns.count; b += blockDim.x) {
+         for (uint32_t b = threadIdx.x; b < ns.count; b += ADJ_THREADS) {
             if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
-               const uint32_t g = gids[ns.off + b];
                uint32_t x, by, bz;
-               block_xyz(mesh, g, x, by, bz);
-               const int y = (int)by, z = (int)bz;
-               const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+               block_xyz(mesh, gids[ns.off + b], x, by, bz);
+               const uint32_t r = (uint32_t)(((int)bz - z0) * ny + ((int)by - y0));
                atomicOr(&H[3 * r + (x >> 5)], 1u << (x & 31));
             }
          }
@@ -391,24 +442,25 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
       base_r += __popc(H[3 * r]) + __popc(H[3 * r + 1]) + __popc(H[3 * r + 2]);
    }
    if (threadIdx.x == 0) {
-      const uint32_t base = atomicAdd(&counters->dst_top, total);
-      s_base = base;
-      if ((uint64_t)base + total > out_capacity) s_flags |= VLGPU_CELL_NOMEM;
+      const uint32_t ob = atomicAdd(&counters->dst_top, total);
+      s_base = ob;
+      if ((uint64_t)ob + total > out_capacity) s_flags |= VLGPU_CELL_NOMEM;
    }
    __syncthreads();
    const bool ok = !(s_flags & VLGPU_CELL_NOMEM);
+   const uint32_t obase = s_base;
    if (ok) {
       // emit the new list in global-ID order; data indices default to "added"
       for (uint32_t r = r0; r < r1; ++r) {
          const uint32_t yy = (uint32_t)(y0 + (int)(r % ny)), zz = (uint32_t)(z0 + (int)(r / ny));
-         uint32_t o = s_base + prefix[r];
+         const uint32_t row_gid = L0 * (yy + L1 * zz);
+         uint32_t o = obase + prefix[r];
          for (int w = 0; w < 3; ++w) {
             uint32_t m = H[3 * r + w];
             while (m) {
                const int bit = __ffs(m) - 1;
                m &= m - 1;
-               const uint32_t x = (uint32_t)(w * 32 + bit);
-               out_gids[o] = x + L0 * (yy + L1 * zz);
+               out_gids[o] = row_gid + (uint32_t)(w * 32 + bit);
                out_src[o] = NO_BLOCK;
                ++o;
             }
@@ -418,39 +470,55 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    __syncthreads();
    // old blocks: kept ones point the new entry at their data, removed ones
    // feed the density loss
-   double lsum = 0.0;
-   for (uint32_t b = threadIdx.x; b < s.count; b += blockDim.x) {
-      const uint32_t g = gids[s.off + b];
-      const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-      uint32_t x, by, bz;
-      block_xyz(mesh, g, x, by, bz);
-      const int y = (int)by, z = (int)bz;
-      bool inH = false;
-      uint32_t pos = 0;
-      if (any && y >= y0 && y <= y1 && z >= z0 && z <= z1) {
-         const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
-         inH = (H[3 * r + (x >> 5)] >> (x & 31)) & 1u;
-         pos = prefix[r] + (uint32_t)mask_popc_below(&H[3 * r], x);
+   double lsum = 0.0;  // sum f of the removed blocks (times dv3 below)
+   for (uint32_t b0 = warp * 32; b0 < s.count; b0 += ADJ_THREADS * ADJ_UNROLL) {
+      uint32_t gg[ADJ_UNROLL], ii[ADJ_UNROLL];
+#pragma unroll
+      for (int u = 0; u < ADJ_UNROLL; ++u) {
+         const uint32_t b = b0 + ADJ_THREADS * u + lane;
+         gg[u] = b < s.count ? gids[s.off + b] : 0u;
+         ii[u] = b < s.count ? (src_index ? src_index[s.off + b] : s.off + b) : NO_BLOCK;
       }
-      if (inH) {
-         if (ok) out_src[s_base + pos] = idx;
-      } else if (idx != NO_BLOCK) {
-         const float* blk = data + (size_t)idx * WID3;
-         double sum = 0.0;
-         for (int q = 0; q < WID3; ++q) sum += (double)blk[q];
-         lsum += dv3 * sum;
+#pragma unroll
+      for (int u = 0; u < ADJ_UNROLL; ++u) {
+         const bool valid = b0 + ADJ_THREADS * u + lane < s.count;
+         uint32_t x, by, bz;
+         block_xyz(mesh, gg[u], x, by, bz);
+         const int y = (int)by, z = (int)bz;
+         bool inH = false;
+         uint32_t pos = 0;
+         if (valid && any && y >= y0 && y <= y1 && z >= z0 && z <= z1) {
+            const uint32_t r = (uint32_t)((z - z0) * ny + (y - y0));
+            inH = (H[3 * r + (x >> 5)] >> (x & 31)) & 1u;
+            pos = prefix[r] + (uint32_t)mask_popc_below(&H[3 * r], x);
+         }
+         if (inH && ok) out_src[obase + pos] = ii[u];
+         // removed blocks, two at a time: each half-warp sums one block's 64
+         // values as float4 rows
+         for (uint32_t rem = __ballot_sync(FULL, valid && !inH && ii[u] != NO_BLOCK); rem;) {
+            const int l0 = __ffs(rem) - 1;
+            rem &= rem - 1;
+            const int l1 = rem ? __ffs(rem) - 1 : -1;
+            if (rem) rem &= rem - 1;
+            const int from = (lane < 16) ? l0 : l1;
+            const uint32_t idx = __shfl_sync(FULL, ii[u], from < 0 ? 0 : from);
+            if (from >= 0) {
+               const float4 v = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx * WID3) + (lane & 15));
+               lsum += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
+            }
+         }
       }
    }
    // CTA sum of the removed mass
 #pragma unroll
-   for (int o = 16; o >= 1; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-   if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = lsum;
+   for (int o = 16; o >= 1; o >>= 1) lsum += __shfl_xor_sync(FULL, lsum, o);
+   if (lane == 0) s_loss[warp] = lsum;
    __syncthreads();
    if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < ADJ_THREADS / 32; ++w) t += s_loss[w];
-      loss[cell] += t;
-      out_slots[cell] = ok ? CellSlot{s_base, total} : CellSlot{0u, 0u};
+      loss[cell] += dv3 * t;
+      out_slots[cell] = ok ? CellSlot{obase, total} : CellSlot{0u, 0u};
       if (s_flags) atomicOr(&status[cell], s_flags);
       if (!ok) atomicOr(&counters->overflow, 1u);
    }
@@ -458,352 +526,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjust_kernel(
    }
 }
 
-// Warp-per-cell adjustment: the result of adjust_kernel (the same block set,
-// list order, data indices and removed mass per block), with one warp per
-// cell, eight cells in flight per CTA and no CTA barrier.  Cells are taken
-// from a counter, so large and small cells balance over the warps.  The
-// dilated set H is built directly: every content block ORs its x-dilated bits
-// into the (2w+1)^2 rows around it, and lanes whose blocks share a row (a run
-// of the list along x) first combine their bits, so such a run costs one OR
-// per target word.  H and the per-row output prefix (16 bits: a cell handled
-// here has at most AW_ROWS * 96 < 65536 blocks) live in the warp's slice of
-// shared memory; a cell whose dilated box has more rows is queued for
-// adjust_kernel.
-constexpr int AW_WARPS = 8;
-constexpr uint32_t AW_ROWS = 600;
-struct AwNeighbour {
-   uint32_t first;  // first mask-row item of the neighbour
-   int32_t y0, z0;
-   uint32_t my, off;
-};
-constexpr size_t AW_WARP_BYTES =
-   AW_ROWS * (3 * sizeof(uint32_t) + sizeof(uint16_t)) + 27 * sizeof(AwNeighbour);
-static_assert(AW_ROWS * 96 < 65536, "16-bit row prefix");
-static_assert((AW_ROWS * (3 * sizeof(uint32_t) + sizeof(uint16_t))) % 4 == 0, "neighbour table alignment");
-
-// Bits [lo, hi] of a 96-bit row that fall in word w (0 <= lo, hi < 96).
-__device__ __forceinline__ uint32_t row_bits(int lo, int hi, int w) {
-   const int a = max(lo - 32 * w, 0), b = min(hi - 32 * w, 31);
-   if (a > b) return 0u;
-   const uint32_t upto = (b == 31) ? 0xffffffffu : ((2u << b) - 1u);
-   return upto & ~((1u << a) - 1u);
-}
-
-// ORs the x-dilated row bits (p0, p1, p2) of a block at row (y, z) into the
-// rows (y + dy, z + dz), |dy|, |dz| <= w, that lie in the box; one lane.
-__device__ __forceinline__ void or_dilated(uint32_t* H, uint32_t p0, uint32_t p1, uint32_t p2, int y, int z, int w,
-                                           int by0, int by1, int bz0, int bz1, int ny) {
-   for (int dz = -w; dz <= w; ++dz) {
-      const int zz = z + dz;
-      if (zz < bz0 || zz > bz1) continue;
-      for (int dy = -w; dy <= w; ++dy) {
-         const int yy = y + dy;
-         if (yy < by0 || yy > by1) continue;
-         uint32_t* dst = &H[3 * (uint32_t)((zz - bz0) * ny + (yy - by0))];
-         if (p0) atomicOr(dst, p0);
-         if (p1) atomicOr(dst + 1, p1);
-         if (p2) atomicOr(dst + 2, p2);
-      }
-   }
-}
-
-__global__ void __launch_bounds__(AW_WARPS * 32) adjust_warp_kernel(
-   const uint32_t* __restrict__ gids, const uint32_t* __restrict__ src_index, const CellSlot* __restrict__ slots,
-   const uint8_t* __restrict__ content, const float* __restrict__ data, const int32_t* __restrict__ neighbors,
-   uint32_t* __restrict__ out_gids, uint32_t* __restrict__ out_src, CellSlot* __restrict__ out_slots,
-   double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
-   uint32_t* __restrict__ wide_cells, uint32_t out_capacity, MeshDev mesh, double min_value, int add_width,
-   double dv3, uint32_t n_cells, const MaskRec* __restrict__ masks, const uint32_t* __restrict__ pool) {
-   extern __shared__ __align__(16) unsigned char aw_smem[];
-   constexpr uint32_t FULL = 0xffffffffu;
-   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   uint32_t* const H = reinterpret_cast<uint32_t*>(aw_smem + (size_t)warp * AW_WARP_BYTES);
-   uint16_t* const prefix = reinterpret_cast<uint16_t*>(H + 3 * AW_ROWS);
-   AwNeighbour* const nbt = reinterpret_cast<AwNeighbour*>(prefix + AW_ROWS);
-   const int L0 = (int)mesh.len[0], L1 = (int)mesh.len[1], L2 = (int)mesh.len[2];
-   const int w = add_width;
-   const int span = 2 * w + 1, n_targets = 3 * span * span;
-   const uint32_t xmask2 = (L0 >= 96) ? 0xffffffffu : ((L0 <= 64) ? 0u : ((1u << (L0 - 64)) - 1u));
-   const uint32_t xmask1 = (L0 >= 64) ? 0xffffffffu : ((L0 <= 32) ? 0u : ((1u << (L0 - 32)) - 1u));
-   const uint32_t xmask0 = (L0 >= 32) ? 0xffffffffu : ((1u << L0) - 1u);
-   for (;;) {
-      uint32_t cell = 0;
-      if (lane == 0) cell = atomicAdd(&counters->adj_cell, 1u);
-      cell = __shfl_sync(FULL, cell, 0);
-      if (cell >= n_cells) break;
-      const CellSlot s = slots[cell];
-      // lanes 0-25: the neighbours' mask records (a missing neighbour reads as
-      // empty), lane 26: the cell's own; without masks every list is walked
-      int32_t nc = -1;
-      if (neighbors && lane < 26) nc = neighbors[(size_t)cell * 26 + lane];
-      if (lane == 26) nc = (int32_t)cell;
-      MaskRec rec{0, -1, 0, -1, NO_MASK, {0u, 0u, 0u}};
-      if (masks && lane < 27) rec = (nc >= 0) ? masks[nc] : MaskRec{0, -1, 0, -1, 0u, {0u, 0u, 0u}};
-      const uint32_t own_off = __shfl_sync(FULL, rec.off, 26);
-      const bool own_mask = own_off != NO_MASK;
-      // pass 1: bounding boxes (y, z) of the cell's content and of its
-      // neighbours' content
-      int y0, y1, z0, z1;
-      if (own_mask) {
-         y0 = __shfl_sync(FULL, rec.y0, 26);
-         y1 = __shfl_sync(FULL, rec.y1, 26);
-         z0 = __shfl_sync(FULL, rec.z0, 26);
-         z1 = __shfl_sync(FULL, rec.z1, 26);
-      } else {
-         y0 = 1 << 20, y1 = -1, z0 = 1 << 20, z1 = -1;
-         for (uint32_t b = lane; b < s.count; b += 32) {
-            if (list_block_content(src_index, content, data, s.off + b, min_value)) {
-               uint32_t bx, by, bz;
-               block_xyz(mesh, gids[s.off + b], bx, by, bz);
-               y0 = min(y0, (int)by); y1 = max(y1, (int)by);
-               z0 = min(z0, (int)bz); z1 = max(z1, (int)bz);
-            }
-         }
-         y0 = __reduce_min_sync(FULL, y0); y1 = __reduce_max_sync(FULL, y1);
-         z0 = __reduce_min_sync(FULL, z0); z1 = __reduce_max_sync(FULL, z1);
-      }
-      int ny0 = 1 << 20, ny1 = -1, nz0 = 1 << 20, nz1 = -1;
-      uint32_t walk = 0;  // neighbours without a stored mask (lane bits)
-      if (neighbors) {
-         if (lane < 26 && rec.off != NO_MASK && rec.y1 >= 0) {
-            ny0 = rec.y0; ny1 = rec.y1; nz0 = rec.z0; nz1 = rec.z1;
-         }
-         walk = __ballot_sync(FULL, lane < 26 && nc >= 0 && rec.off == NO_MASK);
-         for (uint32_t wk = walk; wk; wk &= wk - 1) {
-            const int32_t n = __shfl_sync(FULL, nc, __ffs(wk) - 1);
-            const CellSlot ns = slots[n];
-            for (uint32_t b = lane; b < ns.count; b += 32) {
-               if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
-                  uint32_t bx, by, bz;
-                  block_xyz(mesh, gids[ns.off + b], bx, by, bz);
-                  ny0 = min(ny0, (int)by); ny1 = max(ny1, (int)by);
-                  nz0 = min(nz0, (int)bz); nz1 = max(nz1, (int)bz);
-               }
-            }
-         }
-         ny0 = __reduce_min_sync(FULL, ny0); ny1 = __reduce_max_sync(FULL, ny1);
-         nz0 = __reduce_min_sync(FULL, nz0); nz1 = __reduce_max_sync(FULL, nz1);
-      }
-      const bool own_any = y1 >= 0, nb_any = ny1 >= 0;
-      const bool any = own_any || nb_any;
-      int by0 = 1 << 20, by1 = -1, bz0 = 1 << 20, bz1 = -1;
-      if (own_any) {
-         by0 = max(0, y0 - w); by1 = min(L1 - 1, y1 + w);
-         bz0 = max(0, z0 - w); bz1 = min(L2 - 1, z1 + w);
-      }
-      if (nb_any) {
-         by0 = min(by0, ny0); by1 = max(by1, ny1);
-         bz0 = min(bz0, nz0); bz1 = max(bz1, nz1);
-      }
-      if (!any) { by0 = 0; by1 = -1; bz0 = 0; bz1 = -1; }
-      const int ny = by1 - by0 + 1;
-      const uint32_t rows = any ? (uint32_t)(ny * (bz1 - bz0 + 1)) : 0u;
-      if (rows > AW_ROWS) {
-         if (lane == 0) wide_cells[atomicAdd(&counters->adj_wide, 1u)] = cell;
-         continue;
-      }
-      for (uint32_t q = lane; q < 3 * rows; q += 32) H[q] = 0u;
-      __syncwarp();
-      // pass 2: H = the cell's content dilated by +-w in x, y and z
-      if (own_any && own_mask) {
-         const int my = y1 - y0 + 1;
-         const uint32_t mrows = (uint32_t)(my * (z1 - z0 + 1));
-         for (uint32_t mr = lane; mr < mrows; mr += 32) {
-            const uint32_t* src = pool + own_off + 3 * mr;
-            const uint32_t c0 = __ldg(src), c1 = __ldg(src + 1), c2 = __ldg(src + 2);
-            if (!(c0 | c1 | c2)) continue;
-            uint32_t h0 = c0, h1 = c1, h2 = c2;
-            for (int sft = 1; sft <= w; ++sft) {
-               h0 |= shl96(c0, c1, c2, 0, sft) | shr96(c0, c1, c2, 0, sft);
-               h1 |= shl96(c0, c1, c2, 1, sft) | shr96(c0, c1, c2, 1, sft);
-               h2 |= shl96(c0, c1, c2, 2, sft) | shr96(c0, c1, c2, 2, sft);
-            }
-            or_dilated(H, h0 & xmask0, h1 & xmask1, h2 & xmask2, y0 + (int)(mr % (uint32_t)my),
-                       z0 + (int)(mr / (uint32_t)my), w, by0, by1, bz0, bz1, ny);
-         }
-      } else if (own_any) {
-         for (uint32_t base = 0; base < s.count; base += 32) {
-            const uint32_t b = base + lane;
-            bool c = false;
-            uint32_t x = 0, y = 0, z = 0;
-            if (b < s.count && list_block_content(src_index, content, data, s.off + b, min_value)) {
-               block_xyz(mesh, gids[s.off + b], x, y, z);
-               c = true;
-            }
-            const int lo = max((int)x - w, 0), hi = min((int)x + w, L0 - 1);
-            const uint32_t p0 = c ? row_bits(lo, hi, 0) : 0u, p1 = c ? row_bits(lo, hi, 1) : 0u,
-                           p2 = c ? row_bits(lo, hi, 2) : 0u;
-            // lanes of one row: four or more combine their bits, the rest OR alone
-            const uint32_t key = c ? (z * (uint32_t)L1 + y) : 0xffffffffu;
-            const uint32_t match = __match_any_sync(FULL, key);
-            const bool big = c && __popc(match) >= 4;
-            if (c && !big) or_dilated(H, p0, p1, p2, (int)y, (int)z, w, by0, by1, bz0, bz1, ny);
-            for (uint32_t leaders = __ballot_sync(FULL, big && (int)lane == __ffs(match) - 1); leaders;
-                 leaders &= leaders - 1) {
-               const int leader = __ffs(leaders) - 1;
-               const bool mine = (__shfl_sync(FULL, match, leader) >> lane) & 1u;
-               const uint32_t q0 = __reduce_or_sync(FULL, mine ? p0 : 0u);
-               const uint32_t q1 = __reduce_or_sync(FULL, mine ? p1 : 0u);
-               const uint32_t q2 = __reduce_or_sync(FULL, mine ? p2 : 0u);
-               const int ly = (int)__shfl_sync(FULL, y, leader), lz = (int)__shfl_sync(FULL, z, leader);
-               // one OR per target word, spread over the lanes
-               for (int t = (int)lane; t < n_targets; t += 32) {
-                  const int word = t % 3, d = t / 3;
-                  const int yy = ly + d % span - w, zz = lz + d / span - w;
-                  const uint32_t bits = word == 0 ? q0 : (word == 1 ? q1 : q2);
-                  if (bits && yy >= by0 && yy <= by1 && zz >= bz0 && zz <= bz1)
-                     atomicOr(&H[3 * (uint32_t)((zz - bz0) * ny + (yy - by0)) + word], bits);
-               }
-            }
-         }
-      }
-      // blocks with content in a spatial neighbour (adjust_velocity_blocks,
-      // spatial_cell_cpu.cpp:211-221)
-      if (neighbors && nb_any) {
-         if (masks) {
-            // one item per mask row of every neighbour that has a mask
-            const uint32_t cnt = (lane < 26 && rec.off != NO_MASK && rec.y1 >= 0)
-                                    ? (uint32_t)((rec.y1 - rec.y0 + 1) * (rec.z1 - rec.z0 + 1))
-                                    : 0u;
-            uint32_t incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-               const uint32_t v = __shfl_up_sync(FULL, incl, o);
-               if ((int)lane >= o) incl += v;
-            }
-            const uint32_t items = __shfl_sync(FULL, incl, 31);
-            if (lane < 26)
-               nbt[lane] = AwNeighbour{incl - cnt, rec.y0, rec.z0, (uint32_t)(rec.y1 - rec.y0 + 1), rec.off};
-            if (lane == 26) nbt[26].first = items;
-            __syncwarp();
-            int q = 0;
-            for (uint32_t it = lane; it < items; it += 32) {
-               while (it >= nbt[q + 1].first) ++q;
-               const AwNeighbour m = nbt[q];
-               const uint32_t mr = it - m.first;
-               const uint32_t mz = mr / m.my;
-               const int y = m.y0 + (int)(mr - mz * m.my), z = m.z0 + (int)mz;
-               const uint32_t* src = pool + m.off + 3 * mr;
-               const uint32_t w0 = __ldg(src), w1 = __ldg(src + 1), w2 = __ldg(src + 2);
-               uint32_t* dst = &H[3 * (uint32_t)((z - bz0) * ny + (y - by0))];
-               if (w0) atomicOr(dst, w0);
-               if (w1) atomicOr(dst + 1, w1);
-               if (w2) atomicOr(dst + 2, w2);
-            }
-         }
-         for (uint32_t wk = walk; wk; wk &= wk - 1) {
-            const int32_t n = __shfl_sync(FULL, nc, __ffs(wk) - 1);
-            const CellSlot ns = slots[n];
-            for (uint32_t b = lane; b < ns.count; b += 32) {
-               if (list_block_content(src_index, content, data, ns.off + b, min_value)) {
-                  uint32_t x, y, z;
-                  block_xyz(mesh, gids[ns.off + b], x, y, z);
-                  const uint32_t r = (uint32_t)(((int)z - bz0) * ny + ((int)y - by0));
-                  atomicOr(&H[3 * r + (x >> 5)], 1u << (x & 31));
-               }
-            }
-         }
-      }
-      __syncwarp();
-      // output positions: an exclusive scan of the rows' block counts
-      uint32_t carry = 0;
-      for (uint32_t r0 = 0; r0 < rows; r0 += 32) {
-         const uint32_t r = r0 + lane;
-         const uint32_t c = (r < rows) ? __popc(H[3 * r]) + __popc(H[3 * r + 1]) + __popc(H[3 * r + 2]) : 0u;
-         uint32_t incl = c;
-#pragma unroll
-         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(FULL, incl, o);
-            if ((int)lane >= o) incl += v;
-         }
-         if (r < rows) prefix[r] = (uint16_t)(carry + incl - c);
-         carry += __shfl_sync(FULL, incl, 31);
-      }
-      const uint32_t total = carry;
-      uint32_t obase = 0;
-      if (lane == 0) obase = atomicAdd(&counters->dst_top, total);
-      obase = __shfl_sync(FULL, obase, 0);
-      const bool ok = (uint64_t)obase + total <= out_capacity;
-      __syncwarp();
-      if (ok) {
-         // the new list in global-ID order; data indices default to "added"
-         for (uint32_t r = lane; r < rows; r += 32) {
-            const uint32_t yy = (uint32_t)by0 + r % (uint32_t)ny, zz = (uint32_t)bz0 + r / (uint32_t)ny;
-            const uint32_t row_gid = (uint32_t)L0 * (yy + (uint32_t)L1 * zz);
-            uint32_t o = obase + prefix[r];
-            for (int wd = 0; wd < 3; ++wd) {
-               uint32_t m = H[3 * r + wd];
-               while (m) {
-                  const int bit = __ffs(m) - 1;
-                  m &= m - 1;
-                  out_gids[o] = row_gid + (uint32_t)(wd * 32 + bit);
-                  out_src[o] = NO_BLOCK;
-                  ++o;
-               }
-            }
-         }
-      }
-      __syncwarp();
-      // old blocks: kept ones point the new entry at their data, removed ones
-      // feed the density loss
-      double lsum = 0.0;
-      for (uint32_t b = lane; b < s.count; b += 32) {
-         const uint32_t g = gids[s.off + b];
-         const uint32_t idx = src_index ? src_index[s.off + b] : s.off + b;
-         uint32_t x, by, bz;
-         block_xyz(mesh, g, x, by, bz);
-         const int y = (int)by, z = (int)bz;
-         bool inH = false;
-         uint32_t pos = 0;
-         if (any && y >= by0 && y <= by1 && z >= bz0 && z <= bz1) {
-            const uint32_t r = (uint32_t)((z - bz0) * ny + (y - by0));
-            inH = (H[3 * r + (x >> 5)] >> (x & 31)) & 1u;
-            pos = prefix[r] + (uint32_t)mask_popc_below(&H[3 * r], x);
-         }
-         if (inH) {
-            if (ok) out_src[obase + pos] = idx;
-         } else if (idx != NO_BLOCK) {
-            const float* blk = data + (size_t)idx * WID3;
-            double sum = 0.0;
-            for (int q = 0; q < WID3; ++q) sum += (double)blk[q];
-            lsum += dv3 * sum;
-         }
-      }
-#pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) lsum += __shfl_xor_sync(FULL, lsum, o);
-      if (lane == 0) {
-         loss[cell] += lsum;
-         out_slots[cell] = ok ? CellSlot{obase, total} : CellSlot{0u, 0u};
-         if (!ok) {
-            atomicOr(&status[cell], VLGPU_CELL_NOMEM);
-            atomicOr(&counters->overflow, 1u);
-         }
-      }
-      __syncwarp();  // the warp's next cell reuses its shared memory
-   }
-}
-
-// Rows of (y, z) masks kept in shared memory by adjust_kernel; a cell whose
-// box has more uses its CTA's global scratch slice.  1600 rows (45 KB) leave
-// room for four CTAs of 512 threads per SM.
+// Rows of (y, z) masks kept in shared memory; a cell whose box has more uses
+// its CTA's global scratch slice.  1600 rows (45 KB) leave room for four CTAs
+// per SM.
 constexpr uint32_t ADJ_SMEM_ROWS = 1600;
 size_t adjust_smem_bytes() { return sizeof(uint32_t) * 7 * ADJ_SMEM_ROWS; }
 size_t adjust_scratch_words(const MeshDev& mesh) { return (size_t)7 * mesh.len[1] * mesh.len[2]; }
-constexpr size_t AW_SMEM_BYTES = AW_WARPS * AW_WARP_BYTES;
 
-// CTAs per SM of adjust_kernel (the wide cells)
 int adjust_blocks_per_sm() {
    int n = 0;
    cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adjust_smem_bytes());
    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjust_kernel, ADJ_THREADS, adjust_smem_bytes());
-   return n > 0 ? n : 1;
-}
-
-// CTAs per SM of adjust_warp_kernel
-int adjust_warp_blocks_per_sm() {
-   int n = 0;
-   cudaFuncSetAttribute(adjust_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AW_SMEM_BYTES);
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjust_warp_kernel, AW_WARPS * 32, AW_SMEM_BYTES);
    return n > 0 ? n : 1;
 }
 
@@ -812,14 +545,11 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
-                          uint32_t n_cells, uint32_t* scratch, int grid, int wide_grid, uint32_t* wide_cells,
-                          MaskRec* masks, uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap,
-                          cudaStream_t stream) {
+                          uint32_t n_cells, uint32_t* scratch, int grid, const uint32_t* order, MaskRec* masks,
+                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
    const size_t smem = adjust_smem_bytes();
    cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-   if (e != cudaSuccess) return e;
-   e = cudaFuncSetAttribute(adjust_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AW_SMEM_BYTES);
    if (e != cudaSuccess) return e;
    const bool use_masks = neighbors && masks && pool && pool_top;
    if (use_masks) {
@@ -828,18 +558,13 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
       content_mask_kernel<<<n_cells, MASK_THREADS, 0, stream>>>(gids, src_index, slots, content, data, mesh,
                                                                  min_value, masks, pool, pool_top, pool_cap);
    }
-   // the counters' adj_cell and adj_wide are zero here (the caller clears the
-   // sweep counters before every adjustment)
-   const uint32_t need = (n_cells + AW_WARPS - 1) / AW_WARPS;
-   const uint32_t gw = (uint32_t)grid < need ? (uint32_t)grid : need;
-   adjust_warp_kernel<<<gw, AW_WARPS * 32, AW_SMEM_BYTES, stream>>>(
-      gids, src_index, slots, content, data, neighbors, out_gids, out_src, out_slots, loss, status, counters,
-      wide_cells, out_capacity, mesh, min_value, add_width, dv3, n_cells, use_masks ? masks : nullptr, pool);
-   const uint32_t g = (uint32_t)wide_grid < n_cells ? (uint32_t)wide_grid : n_cells;
+   // the counters' cell_next is zero here (the caller clears the sweep
+   // counters before every adjustment)
+   const uint32_t g = (uint32_t)grid < n_cells ? (uint32_t)grid : n_cells;
    adjust_kernel<<<g, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
                                                     out_src, out_slots, loss, status, counters, out_capacity, mesh,
                                                     min_value, add_width, dv3, n_cells, ADJ_SMEM_ROWS, scratch,
-                                                    use_masks ? masks : nullptr, pool, wide_cells);
+                                                    use_masks ? masks : nullptr, pool, order);
    return cudaGetLastError();
 }
 

@@ -30,6 +30,13 @@ cudaError_t launch_columnize(int dim, const uint32_t* gids, const uint32_t* src_
                              uint32_t dst_capacity, const SweepCell* sweep_cells, uint32_t* status,
                              SweepCounters* counters, BatchStats* stats, const MeshDev& mesh, int wall_margin,
                              uint32_t cell_begin, uint32_t cell_end, int first_of_step, cudaStream_t stream);
+cudaError_t launch_columnize_batch(int dim, const uint32_t* gids, const uint32_t* src_index,
+                                   const CellSlot* src_slots, CellSlot* dst_slots, uint32_t* perm, ColumnSet* sets,
+                                   uint32_t set_capacity, uint32_t dst_capacity, const SweepCell* sweep_cells,
+                                   uint32_t* status, SweepCounters* counters, BatchStats* stats, const MeshDev& mesh,
+                                   int wall_margin, uint32_t n_cells, int first_of_step, uint32_t* wide_cells,
+                                   const uint32_t* order, int wide_grid, cudaStream_t stream);
+int columnize_wide_blocks_per_sm(const MeshDev& mesh);
 cudaError_t launch_remap(int dim, const ColumnSet* sets, SweepCounters* counters, const uint32_t* perm,
                          const float* src_data, float* dst_data, uint32_t* dst_gids, const SweepCell* sweep_cells,
                          uint32_t* status, const MeshDev& mesh, int wall_margin, uint32_t set_capacity,
@@ -61,11 +68,9 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           uint32_t* out_src,
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
-                          uint32_t n_cells, uint32_t* scratch, int grid, int wide_grid, uint32_t* wide_cells,
-                          MaskRec* masks, uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap,
-                          cudaStream_t stream);
+                          uint32_t n_cells, uint32_t* scratch, int grid, const uint32_t* order, MaskRec* masks,
+                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream);
 int adjust_blocks_per_sm();
-int adjust_warp_blocks_per_sm();
 size_t adjust_scratch_words(const MeshDev& mesh);
 cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const CellAccelInputs* in, const MeshDev& mesh,
                           const double vmin[3], const double bs[3], const double dv[3], const double dx[3], double q,
@@ -180,14 +185,16 @@ struct vlgpu_batch {
    TransCounters* tcounters = nullptr;
    int32_t* neighbors = nullptr;  // 26 per cell (-1: none), the spatial neighbours block adjustment consults
    double* dt_buf = nullptr;      // 2 per cell: r-space and v-space time-step limits
-   uint32_t* adj_scratch = nullptr;  // per CTA of the wide-cell adjustment: masks too wide for shared memory
-   uint32_t* adj_wide_cells = nullptr;  // the cells the warp-per-cell adjustment leaves to the wide-cell one
+   uint32_t* adj_scratch = nullptr;  // per adjustment CTA: masks of a cell too wide for shared memory
+   uint32_t* wide_cells = nullptr;  // the cells whose columnize plane is too wide for the capped kernel
+   uint32_t* cell_order = nullptr;  // the cells by decreasing block count at the last upload (persistent kernels)
+   uint32_t* h_order = nullptr;     // pinned staging of cell_order
    vlgpu::MaskRec* mask_recs = nullptr;  // grid: per cell, its content mask record
    uint32_t* mask_pool = nullptr;        // grid: the content mask rows
    uint32_t* mask_top = nullptr;         // grid: words of the pool in use
    uint32_t mask_cap = 0;
-   int adj_grid = 0;       // CTAs of the warp-per-cell adjustment
-   int adj_wide_grid = 0;  // CTAs of the wide-cell adjustment
+   int adj_grid = 0;
+   int col_wide_grid = 0;  // CTAs of the wide-plane columnize
    double* moments_r = nullptr;   // MOM_COUNT per cell: the moments after translation (the "_R" set)
    // pinned staging; each buffer's event marks when its last copy was read
    SweepCell* h_sweep = nullptr;
@@ -196,6 +203,7 @@ struct vlgpu_batch {
    vlgpu::CellSlot* h_slots_out = nullptr;  // n_cells slots of an asynchronous download (mapped pinned)
    vlgpu::CellSlot* d_slots_out = nullptr;  // its device address
    cudaEvent_t ev_sweep = nullptr, ev_accel = nullptr, ev_upload = nullptr, ev_slots = nullptr;
+   cudaEvent_t ev_order = nullptr;  // the last copy of h_order
    // captured step sequences (vlgpu_batch_capture): the executable graph and
    // the buffer state it starts and ends in
    struct GraphSlot {

@@ -48,7 +48,9 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->neighbors);
    cudaFree(b->dt_buf);
    cudaFree(b->adj_scratch);
-   cudaFree(b->adj_wide_cells);
+   cudaFree(b->wide_cells);
+   cudaFree(b->cell_order);
+   if (b->h_order) cudaFreeHost(b->h_order);
    cudaFree(b->mask_recs);
    cudaFree(b->mask_pool);
    cudaFree(b->mask_top);
@@ -61,6 +63,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFreeHost(b->h_slots_in);
    cudaFreeHost(b->h_slots_out);
    if (b->ev_upload) cudaEventDestroy(b->ev_upload);
+   if (b->ev_order) cudaEventDestroy(b->ev_order);
    if (b->ev_slots) cudaEventDestroy(b->ev_slots);
    if (b->ev_sweep) cudaEventDestroy(b->ev_sweep);
    if (b->ev_accel) cudaEventDestroy(b->ev_accel);
@@ -85,9 +88,10 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
    const double thr = b->params.min_value;
    VL_CHECK(cudaMemsetAsync(b->counters, 0, sizeof(SweepCounters), b->stream));
    if (!per_cell) {
-      VL_CHECK(launch_columnize((int)dim, b->st_gids, b->st_src, b->st_slots, b->slots[dst], b->perm, b->sets, cap,
-                                cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm, 0, b->n_cells,
-                                first_of_step ? 1 : 0, b->stream));
+      VL_CHECK(launch_columnize_batch((int)dim, b->st_gids, b->st_src, b->st_slots, b->slots[dst], b->perm, b->sets,
+                                      cap, cap, sweep_cells, b->status, b->counters, b->stats, b->mdev, wm,
+                                      b->n_cells, first_of_step ? 1 : 0, b->wide_cells, b->cell_order,
+                                      b->col_wide_grid, b->stream));
       const bool prof = b->profiling && b->prof_used + 2 <= b->prof_events.size();
       if (prof) VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used], b->stream));
       VL_CHECK(launch_remap((int)dim, b->sets, b->counters, b->perm, b->data[src], b->data[dst], b->gids[dst],
@@ -97,7 +101,7 @@ int sweep_device(vlgpu_batch* b, const SweepCell* sweep_cells, uint32_t dim, boo
          VL_CHECK(cudaEventRecord(b->prof_events[b->prof_used + 1], b->stream));
          b->prof_used += 2;
       }
-      b->launches += 2;
+      b->launches += 3;
       b->remap_launches += 1;
    } else {
       // one columnize + remap launch pair per cell; set and output counters
@@ -162,9 +166,8 @@ int adjust_device(vlgpu_batch* b) {
                           b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
                           (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid,
-                          b->adj_wide_grid, b->adj_wide_cells, b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap,
-                          b->stream));
-   b->launches += (b->neighbors && b->mask_recs) ? 3 : 2;  // content masks first on a grid
+                          b->cell_order, b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, b->stream));
+   b->launches += (b->neighbors && b->mask_recs) ? 2 : 1;  // content masks first on a grid
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
    b->st_gids = b->adj_gids[a];
@@ -361,8 +364,8 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    }
    b->cps_max[0] = remap_blocks_per_sm();
    b->cps_max[1] = moments_blocks_per_sm();
-   b->cps_max[2] = adjust_warp_blocks_per_sm();
-   b->adj_wide_grid = b->sm_count * adjust_blocks_per_sm();
+   b->cps_max[2] = adjust_blocks_per_sm();
+   b->col_wide_grid = b->sm_count * columnize_wide_blocks_per_sm(b->mdev);
    apply_launch(b);
    const uint64_t cap = block_capacity;
    for (int p = 0; p < 2; ++p) {
@@ -402,10 +405,16 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMalloc(&b->stats, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMalloc(&b->rows_used, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMalloc(&b->adj_scratch, sizeof(uint32_t) * adjust_scratch_words(b->mdev) *
-                                            (size_t)std::min<uint32_t>((uint32_t)b->adj_wide_grid, n_cells))) !=
+                                            (size_t)std::min<uint32_t>((uint32_t)b->adj_grid, n_cells))) !=
        cudaSuccess)
       return fail(e, "adjust scratch");
-   if ((e = cudaMalloc(&b->adj_wide_cells, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "adjust");
+   if ((e = cudaMalloc(&b->wide_cells, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "wide");
+   if ((e = cudaMalloc(&b->cell_order, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "order");
+   if ((e = cudaMallocHost(&b->h_order, sizeof(uint32_t) * n_cells)) != cudaSuccess) return fail(e, "order");
+   for (uint32_t c = 0; c < n_cells; ++c) b->h_order[c] = c;
+   if ((e = cudaMemcpy(b->cell_order, b->h_order, sizeof(uint32_t) * n_cells, cudaMemcpyHostToDevice)) !=
+       cudaSuccess)
+      return fail(e, "order");
    if ((e = cudaMemset(b->rows_used, 0, sizeof(uint32_t) * 4)) != cudaSuccess) return fail(e, "rows");
    if ((e = cudaMemset(b->stats, 0, sizeof(BatchStats))) != cudaSuccess) return fail(e, "stats");
    if ((e = cudaMallocHost(&b->h_sweep, sizeof(SweepCell) * n_cells)) != cudaSuccess) return fail(e, "pinned");
@@ -417,6 +426,7 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
       return fail(e, "pinned");
    if ((e = cudaHostGetDevicePointer(&b->d_slots_out, b->h_slots_out, 0)) != cudaSuccess) return fail(e, "pinned");
    if ((e = cudaEventCreateWithFlags(&b->ev_upload, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+   if ((e = cudaEventCreateWithFlags(&b->ev_order, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
    if ((e = cudaEventCreateWithFlags(&b->ev_slots, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
    set_direct_state(b, 0);
    *out = b;
@@ -428,6 +438,22 @@ int vlgpu_batch_destroy(vlgpu_batch* b) {
    if (b->stream) cudaStreamSynchronize(b->stream);
    free_batch(b);
    return VLGPU_OK;
+}
+
+// The cells by decreasing block count, for the warp-per-cell kernels (the
+// longest cells start first).  Waits for the previous copy of the staging
+// buffer, then copies it on the batch's stream.
+static cudaError_t upload_cell_order(vlgpu_batch* b, const uint64_t* offsets) {
+   cudaError_t e = cudaEventSynchronize(b->ev_order);
+   if (e != cudaSuccess) return e;
+   uint32_t* o = b->h_order;
+   for (uint32_t c = 0; c < b->n_cells; ++c) o[c] = c;
+   std::stable_sort(o, o + b->n_cells, [&](uint32_t a, uint32_t c) {
+      return offsets[a + 1] - offsets[a] > offsets[c + 1] - offsets[c];
+   });
+   e = cudaMemcpyAsync(b->cell_order, o, sizeof(uint32_t) * b->n_cells, cudaMemcpyHostToDevice, b->stream);
+   if (e != cudaSuccess) return e;
+   return cudaEventRecord(b->ev_order, b->stream);
 }
 
 int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* gids, const float* data) {
@@ -452,6 +478,7 @@ int vlgpu_batch_upload(vlgpu_batch* b, const uint64_t* offsets, const uint32_t* 
    }
    VL_CHECK(cudaMemcpyAsync(b->slots[0], slots.data(), sizeof(CellSlot) * b->n_cells, cudaMemcpyHostToDevice,
                             b->stream));
+   VL_CHECK(upload_cell_order(b, offsets));
    VL_CHECK(cudaMemsetAsync(b->status, 0, sizeof(uint32_t) * b->n_cells, b->stream));
    VL_CHECK(cudaMemsetAsync(b->loss, 0, sizeof(double) * b->n_cells, b->stream));
    VL_CHECK(cudaStreamSynchronize(b->stream));
@@ -485,6 +512,7 @@ int vlgpu_batch_upload_async(vlgpu_batch* b, const uint64_t* offsets, const uint
       VL_CHECK(cudaMemcpyAsync(b->data[0], data, sizeof(float) * WID3 * total, cudaMemcpyHostToDevice, b->stream));
    }
    VL_CHECK(cudaMemcpyAsync(b->slots[0], hs, sizeof(CellSlot) * b->n_cells, cudaMemcpyHostToDevice, b->stream));
+   VL_CHECK(upload_cell_order(b, offsets));
    VL_CHECK(cudaMemcpyAsync(b->rows_used, &hs[b->n_cells].off, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
    VL_CHECK(cudaMemsetAsync(b->status, 0, sizeof(uint32_t) * b->n_cells, b->stream));
    VL_CHECK(cudaMemsetAsync(b->loss, 0, sizeof(double) * b->n_cells, b->stream));

@@ -121,8 +121,8 @@ struct SweepCounters {
    uint32_t dst_top;
    uint32_t work;
    uint32_t overflow;
-   uint32_t adj_cell;  // block adjustment: next cell a warp takes
-   uint32_t adj_wide;  // block adjustment: cells left to the CTA-per-cell kernel
+   uint32_t cell_next;  // warp-per-cell kernels (columnize, adjustment): next cell a warp takes
+   uint32_t n_wide;     // cells those kernels left to their CTA-per-cell forms
 };
 
 // Running totals kept on the device across sweeps (never reset by a sweep).
