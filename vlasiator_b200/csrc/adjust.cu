@@ -25,13 +25,16 @@
 // its list as before.
 #include <cstdint>
 
+#include "moments_record.cuh"
 #include "vlgpu_common.cuh"
 
 namespace vlgpu {
 
 constexpr int ADJ_THREADS = 256;
-constexpr int ADJ_MIN_CTAS = 4;   // CTAs per SM the register budget is set for
+constexpr int ADJ_MIN_CTAS = 3;   // CTAs per SM the register budget is set for
 constexpr int ADJ_UNROLL = 2;     // list entries per thread in flight
+constexpr uint32_t ADJ_QUEUE = 32 * ADJ_UNROLL;  // old blocks a warp queues per pass
+constexpr uint32_t ADJ_KEPT = 0x80000000u;       // queue flag: the block stays
 constexpr uint32_t NO_BLOCK = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t adj_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
@@ -184,12 +187,16 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
    double* __restrict__ loss, uint32_t* __restrict__ status, SweepCounters* __restrict__ counters,
    uint32_t out_capacity, MeshDev mesh, double min_value, int add_width, double dv3, uint32_t n_cells,
    uint32_t smem_rows, uint32_t* __restrict__ scratch, const MaskRec* __restrict__ masks,
-   const uint32_t* __restrict__ pool, const uint32_t* __restrict__ order) {
+   const uint32_t* __restrict__ pool, const uint32_t* __restrict__ order, double* __restrict__ mom_record,
+   double* __restrict__ pivot, int write_pivot, MomentFrame fr) {
    extern __shared__ uint32_t smem[];
    __shared__ uint32_t warp_sums[32];
    __shared__ int s_box[8];
    __shared__ uint32_t s_base, s_flags, s_item;
    __shared__ double s_loss[ADJ_THREADS / 32];
+   __shared__ double s_mom[ADJ_THREADS / 32][10];            // the warps' moment sums
+   __shared__ uint32_t s_qidx[ADJ_THREADS / 32][ADJ_QUEUE];  // a warp's queue of old blocks: data row
+   __shared__ uint32_t s_qgid[ADJ_THREADS / 32][ADJ_QUEUE];  // and block ID (| ADJ_KEPT when kept)
    __shared__ MaskRec s_rec[27];     // the neighbours' content masks (26: the cell's own)
    __shared__ uint32_t s_first[27];  // first mask-row item of each neighbour
    constexpr uint32_t FULL = 0xffffffffu;
@@ -469,9 +476,28 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
    }
    __syncthreads();
    // old blocks: kept ones point the new entry at their data, removed ones
-   // feed the density loss
+   // feed the density loss; with the moments fused, the kept blocks' values
+   // also give the cell's "_V" moments (MOM_BOTH: the first sums about 0, the
+   // second about the pivot's bulk velocity U)
+   const bool fuse = mom_record != nullptr;
+   double U0 = 0.0, U1 = 0.0, U2 = 0.0;
+   if (fuse) {
+      const double* pv = pivot + (size_t)cell * MOM_COUNT;
+      U0 = pv[MOM_VX]; U1 = pv[MOM_VY]; U2 = pv[MOM_VZ];
+   }
+   // half a warp per queued block, one x-row of four cells per lane
+   const uint32_t half = lane >> 4, sub = lane & 15;
+   const double ox = 0.5 * fr.dv[0], oy = ((sub & 3) + 0.5) * fr.dv[1], oz = ((sub >> 2) + 0.5) * fr.dv[2];
+   const double dv0s = fr.dv[0] * fr.dv[0];
+   double t[10];
+#pragma unroll
+   for (int q = 0; q < 10; ++q) t[q] = 0.0;
    double lsum = 0.0;  // sum f of the removed blocks (times dv3 below)
+   uint32_t* const qidx = s_qidx[warp];
+   uint32_t* const qgid = s_qgid[warp];
+   const uint32_t lanes_below = (1u << lane) - 1u;
    for (uint32_t b0 = warp * 32; b0 < s.count; b0 += ADJ_THREADS * ADJ_UNROLL) {
+      uint32_t qn = 0;
       uint32_t gg[ADJ_UNROLL], ii[ADJ_UNROLL];
 #pragma unroll
       for (int u = 0; u < ADJ_UNROLL; ++u) {
@@ -493,34 +519,99 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
             pos = prefix[r] + (uint32_t)mask_popc_below(&H[3 * r], x);
          }
          if (inH && ok) out_src[obase + pos] = ii[u];
-         // removed blocks, two at a time: each half-warp sums one block's 64
-         // values as float4 rows
-         for (uint32_t rem = __ballot_sync(FULL, valid && !inH && ii[u] != NO_BLOCK); rem;) {
-            const int l0 = __ffs(rem) - 1;
-            rem &= rem - 1;
-            const int l1 = rem ? __ffs(rem) - 1 : -1;
-            if (rem) rem &= rem - 1;
-            const int from = (lane < 16) ? l0 : l1;
-            const uint32_t idx = __shfl_sync(FULL, ii[u], from < 0 ? 0 : from);
-            if (from >= 0) {
-               const float4 v = __ldg(reinterpret_cast<const float4*>(data + (size_t)idx * WID3) + (lane & 15));
-               lsum += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
+         // queue the blocks whose values are read: the removed ones, and with
+         // the moments fused the kept ones too
+         const bool read = valid && ii[u] != NO_BLOCK && (fuse || !inH);
+         const uint32_t bal = __ballot_sync(FULL, read);
+         if (read) {
+            const uint32_t q = qn + __popc(bal & lanes_below);
+            qidx[q] = ii[u];
+            qgid[q] = gg[u] | (inH ? ADJ_KEPT : 0u);
+         }
+         qn += __popc(bal);
+      }
+      __syncwarp();
+      // the queue, eight blocks at a time: half-warp h reads blocks
+      // h, h + 2, h + 4, h + 6, all four rows in flight at once
+      for (uint32_t q0 = 0; q0 < qn; q0 += 8) {
+         float4 f[4];
+         uint32_t gq[4];
+#pragma unroll
+         for (int v = 0; v < 4; ++v) {
+            const uint32_t e = q0 + half + 2 * v;
+            gq[v] = e < qn ? qgid[e] : 0xffffffffu;
+            f[v] = e < qn ? __ldg(reinterpret_cast<const float4*>(data + (size_t)qidx[e] * WID3) + sub)
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+         }
+#pragma unroll
+         for (int v = 0; v < 4; ++v) {
+            if (gq[v] == 0xffffffffu) continue;
+            // the row's sums of f, i f and i^2 f (i = 0..3 along x)
+            const double d0 = f[v].x, d1 = f[v].y, d2 = f[v].z, d3 = f[v].w;
+            const double s0 = (d0 + d1) + (d2 + d3);
+            if (!(gq[v] & ADJ_KEPT)) {
+               lsum += s0;
+               continue;
             }
+            const double s1 = fma(3.0, d3, fma(2.0, d2, d1));
+            const double s2 = fma(9.0, d3, fma(4.0, d2, d1));
+            uint32_t bi, bj, bk;
+            block_xyz(mesh, gq[v] & ~ADJ_KEPT, bi, bj, bk);
+            const double x0 = (fr.vmin[0] + bi * fr.bs[0]) + ox;
+            const double uy = (fr.vmin[1] + bj * fr.bs[1]) + oy;
+            const double uz = (fr.vmin[2] + bk * fr.bs[2]) + oz;
+            const double ds1 = fr.dv[0] * s1;
+            const double sfx = fma(x0, s0, ds1);  // sum f x over the row
+            t[0] += s0;
+            t[1] += sfx;
+            t[2] = fma(s0, uy, t[2]);
+            t[3] = fma(s0, uz, t[3]);
+            // the same row relative to U
+            const double y0 = x0 - U0, vy = uy - U1, vz = uz - U2;
+            const double sfy = fma(y0, s0, ds1);
+            t[4] += fma(y0, fma(y0, s0, 2.0 * ds1), dv0s * s2);
+            const double s0y = s0 * vy;
+            t[5] = fma(s0y, vy, t[5]);
+            t[6] = fma(s0 * vz, vz, t[6]);
+            t[7] = fma(s0y, vz, t[7]);
+            t[8] = fma(sfy, vz, t[8]);
+            t[9] = fma(sfy, vy, t[9]);
          }
       }
+      __syncwarp();  // the queue is refilled
    }
-   // CTA sum of the removed mass
+   // CTA sums of the removed mass and of the moments (fixed order)
 #pragma unroll
    for (int o = 16; o >= 1; o >>= 1) lsum += __shfl_xor_sync(FULL, lsum, o);
    if (lane == 0) s_loss[warp] = lsum;
+   if (fuse) {
+#pragma unroll
+      for (int q = 0; q < 10; ++q) {
+         double v = t[q];
+#pragma unroll
+         for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+         if (lane == 0) s_mom[warp][q] = v;
+      }
+   }
    __syncthreads();
    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < ADJ_THREADS / 32; ++w) t += s_loss[w];
-      loss[cell] += dv3 * t;
+      double tl = 0.0;
+      for (int w = 0; w < ADJ_THREADS / 32; ++w) tl += s_loss[w];
+      loss[cell] += dv3 * tl;
       out_slots[cell] = ok ? CellSlot{obase, total} : CellSlot{0u, 0u};
       if (s_flags) atomicOr(&status[cell], s_flags);
       if (!ok) atomicOr(&counters->overflow, 1u);
+      if (fuse) {
+         double S[10];
+         for (int q = 0; q < 10; ++q) {
+            double v = 0.0;
+            for (int w = 0; w < ADJ_THREADS / 32; ++w) v += s_mom[w][q];
+            S[q] = v;
+         }
+         moments_record<MOM_BOTH>(S, 0.0, 0.0, 0.0, U0, U1, U2, fr.dv[0], fr.dv[1], fr.dv[2], fr.mass, fr.charge,
+                                  mom_record + (size_t)cell * MOM_COUNT,
+                                  write_pivot ? pivot + (size_t)cell * MOM_COUNT : nullptr);
+      }
    }
    __syncthreads();  // the next cell reuses the shared state
    }
@@ -546,7 +637,8 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
                           uint32_t n_cells, uint32_t* scratch, int grid, const uint32_t* order, MaskRec* masks,
-                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream) {
+                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, double* mom_record,
+                          double* pivot, int write_pivot, const MomentFrame& frame, cudaStream_t stream) {
    if (n_cells == 0) return cudaSuccess;
    const size_t smem = adjust_smem_bytes();
    cudaError_t e = cudaFuncSetAttribute(adjust_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -564,7 +656,8 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
    adjust_kernel<<<g, ADJ_THREADS, smem, stream>>>(gids, src_index, slots, content, data, neighbors, out_gids,
                                                     out_src, out_slots, loss, status, counters, out_capacity, mesh,
                                                     min_value, add_width, dv3, n_cells, ADJ_SMEM_ROWS, scratch,
-                                                    use_masks ? masks : nullptr, pool, order);
+                                                    use_masks ? masks : nullptr, pool, order, mom_record, pivot,
+                                                    write_pivot, frame);
    return cudaGetLastError();
 }
 

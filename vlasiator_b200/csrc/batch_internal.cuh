@@ -69,7 +69,8 @@ cudaError_t launch_adjust(const uint32_t* gids, const uint32_t* src_index, const
                           CellSlot* out_slots, double* loss, uint32_t* status, SweepCounters* counters,
                           uint32_t out_capacity, const MeshDev& mesh, double min_value, int add_width, double dv3,
                           uint32_t n_cells, uint32_t* scratch, int grid, const uint32_t* order, MaskRec* masks,
-                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, cudaStream_t stream);
+                          uint32_t* pool, uint32_t* pool_top, uint32_t pool_cap, double* mom_record,
+                          double* pivot, int write_pivot, const MomentFrame& frame, cudaStream_t stream);
 int adjust_blocks_per_sm();
 size_t adjust_scratch_words(const MeshDev& mesh);
 cudaError_t launch_max_dt(const uint32_t* gids, const CellSlot* slots, const CellAccelInputs* in, const MeshDev& mesh,
@@ -165,6 +166,7 @@ struct vlgpu_batch {
    CellAccelInputs* accel_in = nullptr;
    double* moments = nullptr;  // MOM_COUNT per cell
    double* pivot = nullptr;    // MOM_COUNT per cell: first moments (U = 0) the acceleration transform uses
+   double* mom_scratch = nullptr;  // MOM_COUNT per cell: a record for pivots of some cells only
    double* mom_parts = nullptr;   // per cell and part, the part's sums (moments work array)
    uint32_t* mom_done = nullptr;  // per cell, the parts finished (zero between passes)
    int mom_grid = 0;
@@ -242,7 +244,7 @@ void set_direct_state(vlgpu_batch* b, int pool);
 int sweep_device(vlgpu_batch* b, const vlgpu::SweepCell* sweep_cells, uint32_t dim, bool per_cell, bool first_of_step);
 int moments_device(vlgpu_batch* b, bool second, double* record = nullptr, const double* shift = nullptr);
 int moments_both_device(vlgpu_batch* b, double* record);
-int adjust_device(vlgpu_batch* b);
+int adjust_device(vlgpu_batch* b, double* record = nullptr, bool write_pivot = false);
 int materialize(vlgpu_batch* b);
 int materialize_async(vlgpu_batch* b);
 int geometry_device(vlgpu_batch* b, uint32_t map_order);

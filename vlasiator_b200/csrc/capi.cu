@@ -34,6 +34,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->pivot);
    cudaFree(b->mom_parts);
    cudaFree(b->mom_done);
+   cudaFree(b->mom_scratch);
    cudaFree(b->isect12);
    cudaFree(b->loss);
    cudaFree(b->status);
@@ -156,17 +157,30 @@ int moments_both_device(vlgpu_batch* b, double* record) {
    return VLGPU_OK;
 }
 
-int adjust_device(vlgpu_batch* b) {
+// Block adjustment of every cell; with `record`, the same pass also gives the
+// adjusted VDF's "_V" moments (MOM_BOTH: first moments about 0, pressure
+// about the pivot's bulk velocity) into `record`, and with write_pivot its
+// first moments become the next acceleration's pivot.
+int adjust_device(vlgpu_batch* b, double* record, bool write_pivot) {
    const int a = b->adj_next;
    b->adj_next = 1 - a;
    VL_CHECK(cudaMemsetAsync(b->counters, 0, sizeof(SweepCounters), b->stream));
    const double dv3 = b->dv_d[0] * b->dv_d[1] * b->dv_d[2];
+   MomentFrame frame{};
+   for (int d = 0; d < 3; ++d) {
+      frame.vmin[d] = b->vmin_d[d];
+      frame.bs[d] = b->bs_d[d];
+      frame.dv[d] = b->dv_d[d];
+   }
+   frame.mass = b->params.mass;
+   frame.charge = b->params.charge;
    VL_CHECK(launch_adjust(b->st_gids, b->st_src, b->st_slots, b->content_valid ? b->content : nullptr,
                           b->data[b->cur], b->neighbors, b->adj_gids[a], b->adj_src[a], b->adj_slots[a], b->loss,
                           b->status,
                           b->counters, (uint32_t)b->capacity, b->mdev, b->params.min_value,
                           (int)b->params.add_width_v, dv3, b->n_cells, b->adj_scratch, b->adj_grid,
-                          b->cell_order, b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, b->stream));
+                          b->cell_order, b->mask_recs, b->mask_pool, b->mask_top, b->mask_cap, record, b->pivot,
+                          write_pivot ? 1 : 0, frame, b->stream));
    b->launches += (b->neighbors && b->mask_recs) ? 2 : 1;  // content masks first on a grid
    VL_CHECK(cudaMemcpyAsync(b->rows_used + 2 + a, &b->counters->dst_top, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             b->stream));
@@ -175,7 +189,7 @@ int adjust_device(vlgpu_batch* b) {
    b->st_slots = b->adj_slots[a];
    b->st_list = 2 + a;
    b->content_valid = false;
-   b->pivot_valid = false;
+   b->pivot_valid = record && write_pivot;
    return VLGPU_OK;
 }
 
@@ -239,17 +253,10 @@ int accelerate_device(vlgpu_batch* b, uint32_t map_order, bool per_cell, bool ne
       st = sweep_device(b, b->sweep3 + (size_t)d * b->n_cells, d, per_cell, s == 0);
       if (st != VLGPU_OK) return st;
    }
-   // final block adjustment and moments (vlasovmover.cpp:564-569)
-   st = adjust_device(b);
-   if (st != VLGPU_OK) return st;
-   // the "_V" moments: with next_pivot, in one launch with the first moments
-   // of the new VDF as the next step's pivot; else one pass about the pivot
-   // velocity of this step
-   if (!next_pivot) return moments_device(b, true, b->moments, b->pivot);
-   st = moments_both_device(b, b->moments);
-   if (st != VLGPU_OK) return st;
-   b->pivot_valid = true;
-   return VLGPU_OK;
+   // final block adjustment and moments (vlasovmover.cpp:564-569), in one
+   // pass: the "_V" moments of the adjusted VDF, and with next_pivot its first
+   // moments as the next step's pivot
+   return adjust_device(b, b->moments, next_pivot);
 }
 
 // One translation sweep of the whole grid along `dim` (trans_map_1d_amr):
@@ -387,6 +394,7 @@ int vlgpu_batch_create(const vlgpu_mesh* mesh, const vlgpu_params* params, uint3
    if ((e = cudaMalloc(&b->moments, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMemset(b->moments, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMalloc(&b->pivot, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
+   if ((e = cudaMalloc(&b->mom_scratch, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMemset(b->pivot, 0, sizeof(double) * MOM_COUNT * n_cells)) != cudaSuccess) return fail(e, "mom");
    if ((e = cudaMalloc(&b->mom_parts, sizeof(double) * MOM_SUMS_PER_PART * MOM_PARTS_PER_CELL * n_cells)) !=
        cudaSuccess)

@@ -239,7 +239,16 @@ int vlgpu_server_tick(vlgpu_server* s, uint32_t* n_active, uint32_t* n_pending, 
       if (b->st_src) rows[b->cur] = (uint32_t)D;
       VL_CHECK(cudaMemcpyAsync(b->rows_used, rows, sizeof(rows), cudaMemcpyHostToDevice, b->stream));
       b->content_valid = false;
-      b->pivot_valid = false;
+      if (b->pivot_valid && !admitted.empty()) {
+         // the admitted cells' pivots from their VDFs; every other cell keeps
+         // the pivot its last step wrote, so a request's steps do not depend
+         // on the requests admitted beside it
+         const int st = moments_device(b, false, b->mom_scratch);
+         if (st != VLGPU_OK) return st;
+         for (uint32_t c : admitted)
+            VL_CHECK(cudaMemcpyAsync(b->pivot + (size_t)c * MOM_COUNT, b->mom_scratch + (size_t)c * MOM_COUNT,
+                                     sizeof(double) * MOM_COUNT, cudaMemcpyDeviceToDevice, b->stream));
+      }
    }
    for (uint32_t c : admitted) {
       // a new request starts with a clean status word and loss counter

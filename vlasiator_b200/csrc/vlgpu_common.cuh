@@ -109,6 +109,13 @@ __device__ __forceinline__ void block_xyz(const MeshDev& m, uint32_t g, uint32_t
 // bounding box of its content blocks (y1 < 0: none) and the offset of its
 // x-mask rows (3 words per row) in the mask pool, or 0xffffffff when the rows
 // were not stored (the cell's block list is read instead).
+// The velocity mesh in FP64 for the moment sums: minimum, block size and
+// cell size per dimension, and the species' mass and charge.
+struct MomentFrame {
+   double vmin[3], bs[3], dv[3];
+   double mass, charge;
+};
+
 struct MaskRec {
    int32_t y0, y1, z0, z1;
    uint32_t off;
