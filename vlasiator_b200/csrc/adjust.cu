@@ -32,7 +32,7 @@ namespace vlgpu {
 
 constexpr int ADJ_THREADS = 256;
 constexpr int ADJ_MIN_CTAS = 3;   // CTAs per SM the register budget is set for
-constexpr int ADJ_UNROLL = 2;     // list entries per thread in flight
+constexpr int ADJ_UNROLL = 4;     // list entries per thread in flight
 constexpr uint32_t ADJ_QUEUE = 32 * ADJ_UNROLL;  // old blocks a warp queues per pass
 constexpr uint32_t ADJ_KEPT = 0x80000000u;       // queue flag: the block stays
 constexpr uint32_t NO_BLOCK = 0xffffffffu;
@@ -532,10 +532,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
       }
       __syncwarp();
       // the queue, eight blocks at a time: half-warp h reads blocks
-      // h, h + 2, h + 4, h + 6, all four rows in flight at once
-      for (uint32_t q0 = 0; q0 < qn; q0 += 8) {
-         float4 f[4];
-         uint32_t gq[4];
+      // h, h + 2, h + 4, h + 6; the next eight blocks' rows are in flight
+      // while these are summed
+      auto fetch = [&](uint32_t q0, float4* f, uint32_t* gq) {
 #pragma unroll
          for (int v = 0; v < 4; ++v) {
             const uint32_t e = q0 + half + 2 * v;
@@ -543,20 +542,26 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
             f[v] = e < qn ? __ldg(reinterpret_cast<const float4*>(data + (size_t)qidx[e] * WID3) + sub)
                           : make_float4(0.f, 0.f, 0.f, 0.f);
          }
+      };
+      float4 fc[4], fn[4];
+      uint32_t gc[4], gn[4];
+      fetch(0, fc, gc);
+      for (uint32_t q0 = 0; q0 < qn; q0 += 8) {
+         fetch(q0 + 8, fn, gn);
 #pragma unroll
          for (int v = 0; v < 4; ++v) {
-            if (gq[v] == 0xffffffffu) continue;
+            if (gc[v] == 0xffffffffu) continue;
             // the row's sums of f, i f and i^2 f (i = 0..3 along x)
-            const double d0 = f[v].x, d1 = f[v].y, d2 = f[v].z, d3 = f[v].w;
+            const double d0 = fc[v].x, d1 = fc[v].y, d2 = fc[v].z, d3 = fc[v].w;
             const double s0 = (d0 + d1) + (d2 + d3);
-            if (!(gq[v] & ADJ_KEPT)) {
+            if (!(gc[v] & ADJ_KEPT)) {
                lsum += s0;
                continue;
             }
             const double s1 = fma(3.0, d3, fma(2.0, d2, d1));
             const double s2 = fma(9.0, d3, fma(4.0, d2, d1));
             uint32_t bi, bj, bk;
-            block_xyz(mesh, gq[v] & ~ADJ_KEPT, bi, bj, bk);
+            block_xyz(mesh, gc[v] & ~ADJ_KEPT, bi, bj, bk);
             const double x0 = (fr.vmin[0] + bi * fr.bs[0]) + ox;
             const double uy = (fr.vmin[1] + bj * fr.bs[1]) + oy;
             const double uz = (fr.vmin[2] + bk * fr.bs[2]) + oz;
@@ -576,6 +581,11 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_CTAS) adjust_kernel(
             t[7] = fma(s0y, vz, t[7]);
             t[8] = fma(sfy, vz, t[8]);
             t[9] = fma(sfy, vy, t[9]);
+         }
+#pragma unroll
+         for (int v = 0; v < 4; ++v) {
+            fc[v] = fn[v];
+            gc[v] = gn[v];
          }
       }
       __syncwarp();  // the queue is refilled
