@@ -47,11 +47,12 @@ METRIC = "phase-space cell-updates/s (batched vs plain, same GPU); p50/p99 solve
 UNIT = "cell-updates/s"
 WORKLOAD = "batched acceleration, 4096 drifting Maxwellian cells, 1 SLICE-3D step (PPM), dt=0.01 gyroperiod"
 BYTES_PER_CELL_SWEEP = 8  # read + write one fp32 phase-space cell per 1D sweep
-# DRAM bytes (read + write) of one remap launch per source block, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum = 380.0 MB) of the
-# 512-cell case of this workload (705,499 blocks), fused arithmetic; scaled by
-# the source blocks of a launch to give the full-size traffic per launch.
-REMAP_DRAM_BYTES_PER_BLOCK = 380.0e6 / 705499
+# DRAM bytes (read + write) of one remap_walk_kernel launch per source block,
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 203.8 +
+# 175.9 MB) of the 512-cell case of this workload (705,499 blocks at the step's
+# start), fused arithmetic; scaled by the source blocks of a launch to give the
+# full-size traffic per launch.
+REMAP_DRAM_BYTES_PER_BLOCK = 379.7e6 / 705499
 DEFAULT_SEED = 2026  # the workload's seed unless --seed says otherwise
 
 
@@ -444,7 +445,7 @@ def run_ours(args):
                        "what": "device time of one batched acceleration step of all cells"},
         "plain_per_cell": plain,
         "status_cells_flagged": int((status != 0).sum()),
-        "roofline": {"bound": "hbm", "kernel": "remap_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "remap_kernel" if args.exact else "remap_walk_kernel", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": (REMAP_DRAM_BYTES_PER_BLOCK * src_blocks / remap_n) if remap_n else None,
