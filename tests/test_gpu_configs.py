@@ -163,3 +163,33 @@ def test_larmor_ten_steps_match_reference(vl, mesh, exact):
     for s in range(steps):
         lost = (step_loss[s] - (step_loss[s - 1] if s else 0.0)) / dv3
         assert abs(sums[s + 1][0] + lost[0] - sums[s][0]) <= 1e-6 * sums[s][0], f"step {s}"
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_wide_cell_matches_reference(vl, mesh, exact):
+    """A hot cell (T = 60 MK, about 40 x 40 blocks across) among ordinary
+    cells: its transverse planes exceed the columnize launch's shared-memory
+    plane, so its sweeps go through the wide-plane kernel, and its dilated box
+    exceeds the adjustment's shared-memory rows, so it is adjusted with the
+    global scratch masks; one full acceleration step against the reference's."""
+    from vlasiator_b200.projects import maxwellian_cell, random_drifting_cells
+    cells = random_drifting_cells(5, seed=31, mesh=mesh)
+    hot = maxwellian_cell(mesh, 1e6, 6e7, (2e5, -1e5, 1e5))
+    hot.B = np.array([1e-8, 2e-8, -3e-8])
+    cells.append(hot)
+    g = [c.gids for c in cells]
+    d = [c.data for c in cells]
+    L = mesh.length
+    y, z = (hot.gids // L[0]) % L[1], hot.gids // (L[0] * L[1])
+    assert (np.ptp(y) + 1) * (np.ptp(z) + 1) > 1024 and (np.ptp(y) + 3) * (np.ptp(z) + 3) > 1600
+    B = np.stack([c.B for c in cells])
+    dt = 0.01 * 2 * np.pi * MASS_PROTON / (CHARGE * np.linalg.norm(B, axis=1))
+    ref_cells, ref_loss, ref_mom = _reference_steps(mesh, g, d, B, [dt], [1])
+    got = _device_steps(vl, mesh, g, d, B, [dt], [1], exact=exact)
+    if exact:
+        assert _compare(got["cells"], ref_cells, 1e-5) >= len(cells) - 1
+        np.testing.assert_allclose(got["loss"], ref_loss, rtol=1e-9, atol=1e-30)
+        _check_moments(got["moments"], ref_mom, 1e-10, 1e-9)
+    else:
+        _compare(got["cells"], ref_cells, 1e-5)
+        _check_moments(got["moments"], ref_mom, 1e-6, 1e-5)

@@ -157,7 +157,7 @@ __device__ __forceinline__ void set_corners(const SweepCell& P, uint32_t si, uin
 // ---------------------------------------------------------------------------
 // columnize: one CTA per cell
 // ---------------------------------------------------------------------------
-constexpr int COL_THREADS = 512;
+constexpr int COL_THREADS = 256;
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
