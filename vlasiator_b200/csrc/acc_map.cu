@@ -848,7 +848,9 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
          float g1f = (float)(g + 1);   // the pending target's edge index (g + 1)
          uint32_t soff = (uint32_t)(g & RMASK) * 16u;  // the pending target's slot
          float u = fs(e, v_l) * inv_dv;
-         float acc = ring[soff];  // what another column left in the slot
+         // minus the pending target's accumulated mass (kept negated so that
+         // both branches of the per-cell update are one select and one add)
+         float nacc = -ring[soff];  // what another column left in the slot
          float pw0 = 0.0f, pw1 = 0.0f, pw2 = 0.0f, pw3 = 0.0f;  // cells below the block (zero padding)
          float cur[4], nxt[4];
          load_lane<DIM>(src_data, perm[cs.src_pos + src_rank], i, j, cur);
@@ -920,8 +922,8 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                // ---- distribute the cell over the lane's targets ----
                const bool has = u < 1.0f;  // the pending target's right edge lies inside this cell
                float D = recon_integral<RECON>(u, a);  // used only when has
-               if (has) ring[soff] = acc + D;
-               acc = has ? v0 - D : acc + v0;
+               if (has) ring[soff] = D - nacc;
+               nacc = (has ? D : nacc) - v0;
                {
                   const float g1n = g1f + 1.0f;
                   const float un = fs(fa(fm(g1n, dk), im), v_l) * inv_dv;  // the next edge (reference's rounding)
@@ -939,7 +941,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                      soff = (soff + 16u) & SMASK;
                      u = fs(fa(fm(g1f, dk), im), v_l) * inv_dv;
                   }
-                  acc = v0 - D;
+                  nacc = D - v0;
                }
                u -= 1.0f;
                v_l = fa(v_l, dv);
@@ -950,7 +952,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                // column done: the pending target keeps the rest; targets
                // above the column's highest cell are folded into it
                if (g > hi) {
-                  float extra = acc;
+                  float extra = -nacc;
                   for (int t = hi + 1; t < g && t <= hi + RING_CELLS / 2; ++t) {
                      extra += ring[(t & RMASK) * 16];
                      ring[(t & RMASK) * 16] = 0.0f;
@@ -960,8 +962,8 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                   top = hi;
                } else {
                   // the slot holds nothing of this column's yet (its first
-                  // target's earlier content is already in acc)
-                  ring[soff] = acc;
+                  // target's earlier content is already in nacc)
+                  ring[soff] = -nacc;
                   top = g;
                }
             }
