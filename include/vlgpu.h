@@ -109,6 +109,31 @@ int vlgpu_batch_download_begin(vlgpu_batch* b);
 int vlgpu_batch_download_end(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_count, uint32_t* gids, float* data,
                              uint64_t capacity, uint64_t* used);
 
+/* Ghost-cell exchange of a spatial grid split over several batches (one per
+   GPU and rank).  No reference counterpart as an entry point: this is the
+   data movement of the remote-neighbour updates of a distributed grid
+   (update_remote_mapping_contribution_amr, vlasovsolver/cpu_trans_map_amr.cpp:
+   493-810, and dccrg's neighbour-data updates), rebuilt as a pack into a
+   device buffer, a transfer the caller makes (NCCL send/recv or any other)
+   and an unpack into the receiving batch.  Both return after their device
+   work is done.
+
+   vlgpu_batch_pack_cells: the blocks (IDs and 64 values) of cells[0..n_sel)
+   into gids / data, DEVICE buffers on the batch's device of `capacity`
+   blocks, cell after cell; counts (host, n_sel) receives each cell's block
+   count and *used the total (VLGPU_ENOMEM, with *used set, when it exceeds
+   capacity).
+
+   vlgpu_batch_unpack_cells: replaces the blocks of cells[0..n_sel) with
+   counts[i] blocks each, taken cell after cell from gids / data (device
+   buffers on the batch's device, as vlgpu_batch_pack_cells writes them).
+   The blocks are appended behind the rows in use (VLGPU_ENOMEM beyond the
+   batch's capacity); a block ID outside the mesh gives VLGPU_EINVAL. */
+int vlgpu_batch_pack_cells(vlgpu_batch* b, uint32_t n_sel, const uint32_t* cells, uint32_t* counts, uint32_t* gids,
+                           float* data, uint64_t capacity, uint64_t* used);
+int vlgpu_batch_unpack_cells(vlgpu_batch* b, uint32_t n_sel, const uint32_t* cells, const uint32_t* counts,
+                             const uint32_t* gids, const float* data);
+
 /* Per-cell VLGPU_CELL_* bits accumulated since the last upload. */
 int vlgpu_batch_status(vlgpu_batch* b, uint32_t* status);
 

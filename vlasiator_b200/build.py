@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvlgpu.so")
-SOURCES = ["acc_map.cu", "moments_geometry.cu", "adjust.cu", "translate.cu", "fill.cu", "capi.cu", "serve.cu", "noalloc.cu", "launch.cu"]
+SOURCES = ["acc_map.cu", "moments_geometry.cu", "adjust.cu", "translate.cu", "fill.cu", "capi.cu", "serve.cu", "noalloc.cu", "launch.cu", "halo.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "--shared",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-ccbin", "/usr/bin/g++", "-Xptxas", "-warn-spills"]
@@ -23,6 +23,7 @@ def build(verbose: bool = False, extra=()) -> str:
                                                        os.path.join(CSRC, "geometry.cuh"),
                                                        os.path.join(CSRC, "batch_internal.cuh"),
                                                        os.path.join(CSRC, "fused_ppm.cuh"),
+                                                       os.path.join(CSRC, "moments_record.cuh"),
                                                        os.path.join(HERE, "..", "include", "vlgpu.h")])
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
         return LIB

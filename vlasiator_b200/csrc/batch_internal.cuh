@@ -191,6 +191,8 @@ struct vlgpu_batch {
    uint32_t* wide_cells = nullptr;  // the cells whose columnize plane is too wide for the capped kernel
    uint32_t* cell_order = nullptr;  // the cells by decreasing block count at the last upload (persistent kernels)
    uint32_t* h_order = nullptr;     // pinned staging of cell_order
+   uint32_t* halo_scratch = nullptr;  // cell descriptors of a pack / unpack of some cells (grown on demand)
+   size_t halo_words = 0;
    vlgpu::MaskRec* mask_recs = nullptr;  // grid: per cell, its content mask record
    uint32_t* mask_pool = nullptr;        // grid: the content mask rows
    uint32_t* mask_top = nullptr;         // grid: words of the pool in use

@@ -50,6 +50,7 @@ void free_batch(vlgpu_batch* b) {
    cudaFree(b->dt_buf);
    cudaFree(b->adj_scratch);
    cudaFree(b->wide_cells);
+   cudaFree(b->halo_scratch);
    cudaFree(b->cell_order);
    if (b->h_order) cudaFreeHost(b->h_order);
    cudaFree(b->mask_recs);

@@ -80,6 +80,9 @@ SIGNATURES = {
     "vlgpu_batch_block_counts": (ctypes.c_int, [_vp, _u32p]),
     "vlgpu_batch_download": (ctypes.c_int, [_vp, _u64p, _u32p, _fp, ctypes.c_uint64]),
     "vlgpu_batch_status": (ctypes.c_int, [_vp, _u32p]),
+    "vlgpu_batch_pack_cells": (ctypes.c_int, [_vp, ctypes.c_uint32, _u32p, _u32p, _vp, _vp, ctypes.c_uint64,
+                                              _u64p]),
+    "vlgpu_batch_unpack_cells": (ctypes.c_int, [_vp, ctypes.c_uint32, _u32p, _u32p, _vp, _vp]),
     "vlgpu_map_1d": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
     "vlgpu_map_1d_per_cell": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
     "vlgpu_accelerate_with_intersections": (ctypes.c_int, [_vp, _dp, ctypes.c_uint32]),
@@ -183,6 +186,7 @@ class Batch:
         _check(self.lib.vlgpu_batch_create(ctypes.byref(m), ctypes.byref(self.params), self.n_cells, self.capacity,
                                            device, ctypes.byref(h)), "vlgpu_batch_create")
         self.h = h
+        self.device = int(device)
         self._inflight = None  # host arrays an asynchronous upload still reads
         self.set_reconstruction(recon)
         self.set_exact(exact)
@@ -245,6 +249,29 @@ class Batch:
         c = np.zeros(self.n_cells, np.uint32)
         _check(self.lib.vlgpu_batch_block_counts(self.h, _p(c, ctypes.c_uint32)), "vlgpu_batch_block_counts")
         return c
+
+    def pack_cells(self, cells, gids_ptr: int, data_ptr: int, capacity: int):
+        """The blocks of `cells` into device buffers (addresses on the batch's
+        device: capacity uint32 IDs and capacity x 64 floats), cell after cell;
+        returns (block count per cell, blocks written)."""
+        c = np.ascontiguousarray(cells, np.uint32)
+        counts = np.zeros(max(len(c), 1), np.uint32)
+        used = ctypes.c_uint64(0)
+        _check(self.lib.vlgpu_batch_pack_cells(self.h, len(c), _p(c, ctypes.c_uint32), _p(counts, ctypes.c_uint32),
+                                               ctypes.c_void_p(gids_ptr), ctypes.c_void_p(data_ptr), int(capacity),
+                                               ctypes.byref(used)), "vlgpu_batch_pack_cells")
+        return counts[:len(c)], int(used.value)
+
+    def unpack_cells(self, cells, counts, gids_ptr: int, data_ptr: int):
+        """Replaces the blocks of `cells` with counts[i] blocks each, read cell
+        after cell from device buffers (as pack_cells writes them)."""
+        c = np.ascontiguousarray(cells, np.uint32)
+        n = np.ascontiguousarray(counts, np.uint32)
+        if len(c) != len(n):
+            raise ValueError("cells and counts differ in length")
+        _check(self.lib.vlgpu_batch_unpack_cells(self.h, len(c), _p(c, ctypes.c_uint32), _p(n, ctypes.c_uint32),
+                                                 ctypes.c_void_p(gids_ptr), ctypes.c_void_p(data_ptr)),
+               "vlgpu_batch_unpack_cells")
 
     def status(self) -> np.ndarray:
         s = np.zeros(self.n_cells, np.uint32)
