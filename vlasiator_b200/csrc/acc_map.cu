@@ -941,6 +941,9 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                      soff = (soff + 16u) & SMASK;
                      u = fs(fa(fm(g1f, dk), im), v_l) * inv_dv;
                   }
+                  // more than eight target edges in one source cell (dk < dv / 8):
+                  // outside what the walk represents, reported with the cell
+                  range_err |= u < 1.0f;
                   nacc = D - v0;
                }
                u -= 1.0f;
