@@ -191,6 +191,48 @@ __device__ __forceinline__ void ppm_coeff_x2(float2 vm1, float2 v0, float2 vp1, 
    a2 = __ffma2_rn(v0, f2(-2.0f), __fadd2_rn(fl, fr));
 }
 
+// The same PPM in the walk form (that of the acceleration's
+// remap_walk_kernel), for a walk along the cells: what a cell shares with its
+// left neighbour comes in from it instead of being recomputed.
+//  - tl: the left face's test (vm1 - fl)(fl - v0), which is the left
+//    neighbour's right-face test (v0' - fr')(fr' - vp1') with the same
+//    rounded factors; tr returns this cell's, for the next cell.
+//  - dprev: v0 - vm1, the left neighbour's vp1 - v0; dn returns this cell's.
+//  - The superbee slope in closed form, min(2 min(|a|,|b|), max(|a|,|b|)).
+//  - The two Colella-Woodward corrections taken as alternatives: in exact
+//    arithmetic the second cannot fire once the first has.
+// Its limiter decisions are the reference's, up to rounding in the
+// corrections; the fused tolerances cover it.
+__device__ __forceinline__ void ppm_walk_x2(float2 v0, float2 vp1, float2 fl, float2 fr, float2 tl, float2 dprev,
+                                            float2& tr, float2& dn, float2& a0, float2& a1, float2& a2) {
+   dn = p_sub(vp1, v0);
+   tr = __fmul2_rn(p_sub(v0, fr), p_sub(fr, vp1));
+   float2 hs;
+   {
+      const float anx = fabsf(dn.x), apx = fabsf(dprev.x), any = fabsf(dn.y), apy = fabsf(dprev.y);
+      hs.x = copysignf(0.5f * fminf(2.0f * fminf(anx, apx), fmaxf(anx, apx)), dn.x);
+      hs.y = copysignf(0.5f * fminf(2.0f * fminf(any, apy), fmaxf(any, apy)), dn.y);
+   }
+   const float2 nl = p_sub(v0, hs), nr = __fadd2_rn(v0, hs);
+   const bool sx = dn.x * dprev.x > 0.0f, sy = dn.y * dprev.y > 0.0f;
+   float2 l, r;
+   l.x = sx ? (tl.x < 0.0f ? nl.x : fl.x) : v0.x;
+   l.y = sy ? (tl.y < 0.0f ? nl.y : fl.y) : v0.y;
+   r.x = sx ? (tr.x < 0.0f ? nr.x : fr.x) : v0.x;
+   r.y = sy ? (tr.y < 0.0f ? nr.y : fr.y) : v0.y;
+   const float2 d = p_sub(r, l), e = __ffma2_rn(__fadd2_rn(l, r), f2(-0.5f), v0);
+   const float2 de = __fmul2_rn(d, e), dd = __fmul2_rn(d, __fmul2_rn(d, f2((float)(1.0 / 6.0))));
+   const float2 v3 = __fmul2_rn(v0, f2(3.0f));
+   const float2 alt_l = __ffma2_rn(r, f2(-2.0f), v3), alt_r = __ffma2_rn(l, f2(-2.0f), v3);
+   a0.x = (de.x > dd.x) ? alt_l.x : l.x;
+   a0.y = (de.y > dd.y) ? alt_l.y : l.y;
+   float2 nfr;
+   nfr.x = (-dd.x > de.x) ? alt_r.x : r.x;
+   nfr.y = (-dd.y > de.y) ? alt_r.y : r.y;
+   a1 = p_sub(__ffma2_rn(a0, f2(-2.0f), v3), nfr);
+   a2 = __ffma2_rn(v0, f2(-2.0f), __fadd2_rn(a0, nfr));
+}
+
 // Integral of two PPM reconstructions from 0 to u (u * (a0 + u (a1 + u a2))).
 __device__ __forceinline__ float2 ppm_integral_x2(float2 u, float2 a0, float2 a1, float2 a2) {
    return __fmul2_rn(u, __ffma2_rn(u, __ffma2_rn(u, a2, a1), a0));

@@ -428,6 +428,21 @@ __device__ __forceinline__ float2 outgoing_x2(float2 vm1, float2 v0, float2 vp1,
    return make_float2(act_x ? ngbr.x : 0.0f, act_y ? ngbr.y : 0.0f);
 }
 
+// The same in the walk form (ppm_walk_x2): the left-face test and v0 - vm1
+// come in from the cell to the left, and this cell's go out in tl and dprev.
+__device__ __forceinline__ float2 outgoing_walk_x2(float2 v0, float2 vp1, float2 fl, float2 fr, float2& tl,
+                                                   float2& dprev, float2 z1, float2 z2, uint32_t act_x,
+                                                   uint32_t act_y) {
+   float2 a0, a1, a2, tr, dn;
+   ppm_walk_x2(v0, vp1, fl, fr, tl, dprev, tr, dn, a0, a1, a2);
+   tl = tr;
+   dprev = dn;
+   const float2 t2 = __ffma2_rn(z2, __ffma2_rn(z2, a2, a1), a0);
+   const float2 t1 = __ffma2_rn(z1, __ffma2_rn(z1, a2, a1), a0);
+   const float2 ngbr = p_sub(__fmul2_rn(z2, t2), __fmul2_rn(z1, t1));
+   return make_float2(act_x ? ngbr.x : 0.0f, act_y ? ngbr.y : 0.0f);
+}
+
 // This lane's two columns of the block at data index idx (zeros where the
 // cell lacks the block).
 __device__ __forceinline__ float2 load_column_pair(const float* __restrict__ src, uint32_t idx, int lane) {
@@ -547,15 +562,18 @@ __global__ void __launch_bounds__(TF_THREADS, 3) trans_fused_kernel(
          posy |= py << j;
       }
       // the outgoing integrals of cells -1 and 0, the left face of cell 1
-      float2 nb_m1, nb_0, fl;
+      // and, carried along the walk, its left-face test and v0 - vm1
+      float2 nb_m1, nb_0, fl, tl, dprev;
       {
          const uint32_t ax = posx | (posx << 1) | (posx << 2) | (posx >> 1) | (posx >> 2);
          const uint32_t ay = posy | (posy << 1) | (posy << 2) | (posy >> 1) | (posy >> 2);
          const float2 fm1 = h4_face_x2(w[0], w[1], w[2], w[3]);
          const float2 f0 = h4_face_x2(w[1], w[2], w[3], w[4]);
          fl = h4_face_x2(w[2], w[3], w[4], w[5]);
-         nb_m1 = outgoing_x2(w[1], w[2], w[3], fm1, f0, z1, z2, (ax >> 2) & 1u, (ay >> 2) & 1u);
-         nb_0 = outgoing_x2(w[2], w[3], w[4], f0, fl, z1, z2, (ax >> 3) & 1u, (ay >> 3) & 1u);
+         tl = __fmul2_rn(p_sub(w[1], fm1), p_sub(fm1, w[2]));
+         dprev = p_sub(w[2], w[1]);
+         nb_m1 = outgoing_walk_x2(w[2], w[3], fm1, f0, tl, dprev, z1, z2, (ax >> 2) & 1u, (ay >> 2) & 1u);
+         nb_0 = outgoing_walk_x2(w[3], w[4], f0, fl, tl, dprev, z1, z2, (ax >> 3) & 1u, (ay >> 3) & 1u);
       }
 
       for (uint32_t s0 = 0;;) {
@@ -568,8 +586,8 @@ __global__ void __launch_bounds__(TF_THREADS, 3) trans_fused_kernel(
             // cell y = s0+1+i (window i+4): its right face and outgoing integral;
             // then the new value of cell y-1 = s0+i (window i+3)
             const float2 fr = h4_face_x2(w[i + 3], w[i + 4], w[i + 5], w[i + 6]);
-            const float2 nb =
-               outgoing_x2(w[i + 3], w[i + 4], w[i + 5], fl, fr, z1, z2, (ax >> (i + 4)) & 1u, (ay >> (i + 4)) & 1u);
+            const float2 nb = outgoing_walk_x2(w[i + 4], w[i + 5], fl, fr, tl, dprev, z1, z2, (ax >> (i + 4)) & 1u,
+                                               (ay >> (i + 4)) & 1u);
             fl = fr;
             const uint32_t r = (s0 + (uint32_t)i < N) ? trow[s0 + i] : NO_ROW;
             if (r != NO_ROW) {
