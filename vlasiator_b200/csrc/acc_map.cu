@@ -436,6 +436,10 @@ constexpr int REMAP_THREADS = 256;
 constexpr int RING_BLOCKS = 8;               // target blocks held per set
 constexpr int RING_CELLS = RING_BLOCKS * WID;  // per lane
 constexpr int RING_STRIDE = RING_CELLS * 16 + 16;  // floats per half-warp (+16 pad: bank shift)
+// remap_walk_kernel keeps each lane's ring contiguous: 32 cells padded to 36
+// floats, so a block's four cells are one aligned 16-byte access and the
+// lanes of a half-warp touching the same slot fall in 8 distinct bank groups
+constexpr int WALK_LANE_STRIDE = RING_CELLS + 4;
 
 template <int DIM>
 __device__ __forceinline__ int cell_offset(int i, int j, int g) {
@@ -742,11 +746,13 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
    const float* __restrict__ src_data, float* __restrict__ dst_data, uint32_t* __restrict__ dst_gids,
    const SweepCell* __restrict__ sweep_cells, uint32_t* __restrict__ status, MeshDev mesh, int wall_margin,
    uint32_t set_capacity, uint8_t* __restrict__ content_out, double content_threshold) {
-   __shared__ float ring_all[(REMAP_THREADS / 16) * RING_STRIDE];
+   __shared__ __align__(16) float ring_all[REMAP_THREADS * WALK_LANE_STRIDE];
    const int hw = threadIdx.x >> 4;
    const int lane = threadIdx.x & 15;
    const unsigned hmask = 0xffffu << (threadIdx.x & 16);
-   float* ring = ring_all + hw * RING_STRIDE + lane;  // this lane's slots: ring[16 * t]
+   // this lane's slots ring[t], t = target cell mod RING_CELLS, contiguous so
+   // that a target block's four cells are one 16-byte access
+   float* ring = ring_all + (size_t)threadIdx.x * WALK_LANE_STRIDE;
    const int i = lane & 3, j = lane >> 2;
    uint32_t n_sets = *((volatile uint32_t*)&counters->n_sets);
    n_sets = (n_sets < set_capacity) ? n_sets : set_capacity;
@@ -756,10 +762,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
    const float content_thr = __double2float_ru(content_threshold);
    constexpr float one_sixth = (float)(1.0 / 6.0);
    constexpr int RMASK = RING_CELLS - 1;
-   constexpr uint32_t SMASK = RING_CELLS * 16 - 1;  // slot offsets wrap around the ring
+   constexpr uint32_t SMASK = RING_CELLS - 1;  // slot offsets wrap around the ring
 
 #pragma unroll
-   for (int q = 0; q < RING_CELLS; ++q) ring[q * 16] = 0.0f;
+   for (int q = 0; q < RING_CELLS; ++q) ring[q] = 0.0f;
    for (;;) {
       uint32_t sidx = 0;
       if (lane == 0) sidx = atomicAdd(&counters->work, 1u);
@@ -788,13 +794,10 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
 
       auto flush_until = [&](int limit_block) {
          while (next_flush < 96 && next_flush < limit_block) {
-            float v[4];
             const int slot = (next_flush & (RING_BLOCKS - 1)) * WID;
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-               v[g] = ring[(slot + g) * 16];
-               ring[(slot + g) * 16] = 0.0f;
-            }
+            const float4 v4 = *reinterpret_cast<const float4*>(ring + slot);
+            *reinterpret_cast<float4*>(ring + slot) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const float v[4] = {v4.x, v4.y, v4.z, v4.w};
             const uint32_t o = cs.dst_pos + out_idx;
             store_lane<DIM>(dst_data + (size_t)o * WID3, i, j, v);
             const bool c = fmaxf(fmaxf(v[0], v[1]), fmaxf(v[2], v[3])) >= content_thr;
@@ -846,7 +849,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
             e = fa(fm((float)(g + 1), dk), im);
          }
          float g1f = (float)(g + 1);   // the pending target's edge index (g + 1)
-         uint32_t soff = (uint32_t)(g & RMASK) * 16u;  // the pending target's slot
+         uint32_t soff = (uint32_t)(g & RMASK);  // the pending target's slot
          float u = fs(e, v_l) * inv_dv;
          // minus the pending target's accumulated mass (kept negated so that
          // both branches of the per-cell update are one select and one add)
@@ -929,7 +932,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                   const float un = fs(fa(fm(g1n, dk), im), v_l) * inv_dv;  // the next edge (reference's rounding)
                   g1f = has ? g1n : g1f;
                   u = has ? un : u;
-                  soff = has ? ((soff + 16u) & SMASK) : soff;
+                  soff = has ? ((soff + 1u) & SMASK) : soff;
                }
                if (u < 1.0f) {
                   // further edges inside the same source cell (dk < dv)
@@ -938,7 +941,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                      ring[soff] = D2 - D;
                      D = D2;
                      g1f += 1.0f;
-                     soff = (soff + 16u) & SMASK;
+                     soff = (soff + 1u) & SMASK;
                      u = fs(fa(fm(g1f, dk), im), v_l) * inv_dv;
                   }
                   // more than eight target edges in one source cell (dk < dv / 8):
@@ -957,11 +960,11 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
                if (g > hi) {
                   float extra = -nacc;
                   for (int t = hi + 1; t < g && t <= hi + RING_CELLS / 2; ++t) {
-                     extra += ring[(t & RMASK) * 16];
-                     ring[(t & RMASK) * 16] = 0.0f;
+                     extra += ring[t & RMASK];
+                     ring[t & RMASK] = 0.0f;
                   }
                   range_err |= g > hi + RING_CELLS / 2;
-                  ring[(hi & RMASK) * 16] += extra;
+                  ring[hi & RMASK] += extra;
                   top = hi;
                } else {
                   // the slot holds nothing of this column's yet (its first
@@ -996,7 +999,7 @@ __global__ void __launch_bounds__(REMAP_THREADS, RECON == RECON_PQM ? 2 : 4) rem
       if (__any_sync(hmask, range_err)) {
          if (lane == 0) atomicOr(&status[cs.cell], VLGPU_CELL_RANGE);
 #pragma unroll
-         for (int q = 0; q < RING_CELLS; ++q) ring[q * 16] = 0.0f;
+         for (int q = 0; q < RING_CELLS; ++q) ring[q] = 0.0f;
       }
    }
 }
