@@ -121,7 +121,7 @@ def test_one_slab_with_wrapped_ghosts_matches_the_whole_grid(whole_grid):
 def test_two_slabs_match_the_whole_grid(whole_grid):
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that holds CUDA
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)

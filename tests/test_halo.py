@@ -117,7 +117,7 @@ def test_slab_bookkeeping():
 @pytest.mark.parametrize("world", [2, 3])
 def test_ghost_exchange_and_sharded_translation(world):
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that holds CUDA
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, DIMS, out), nprocs=world, join=True)
         res = dict(out)

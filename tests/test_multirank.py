@@ -35,7 +35,7 @@ def _rank_main(rank, world, port, out):
 def test_two_gloo_ranks_shard_and_reduce():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that holds CUDA
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
