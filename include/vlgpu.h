@@ -128,7 +128,12 @@ int vlgpu_batch_download_end(vlgpu_batch* b, uint32_t* cell_off, uint32_t* cell_
    counts[i] blocks each, taken cell after cell from gids / data (device
    buffers on the batch's device, as vlgpu_batch_pack_cells writes them).
    The blocks are appended behind the rows in use (VLGPU_ENOMEM beyond the
-   batch's capacity); a block ID outside the mesh gives VLGPU_EINVAL. */
+   batch's capacity); a block ID outside the mesh gives VLGPU_EINVAL.
+
+   Both work on the batch's own stream, which waits for no other stream, and
+   return once it is idle.  So the caller's buffers must be complete before
+   the call (synchronise the stream that received or last used them), and
+   they are free to reuse when it returns. */
 int vlgpu_batch_pack_cells(vlgpu_batch* b, uint32_t n_sel, const uint32_t* cells, uint32_t* counts, uint32_t* gids,
                            float* data, uint64_t capacity, uint64_t* used);
 int vlgpu_batch_unpack_cells(vlgpu_batch* b, uint32_t n_sel, const uint32_t* cells, const uint32_t* counts,

@@ -95,12 +95,19 @@ class BatchSide:
         cap = int(counts_all[np.asarray(cells, np.int64)].sum())
         g = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
         d = torch.empty((max(cap, 1), 64), dtype=torch.float32, device=self.device)
+        # torch may hand out memory that its own stream still reads; the batch
+        # writes it on its stream, which waits for no other
+        torch.cuda.current_stream(self.device).synchronize()
         counts, used = self.batch.pack_cells(cells, g.data_ptr(), d.data_ptr(), cap)
         return counts.astype(np.int32), g[:used], d[:used]
 
     def import_(self, cells, counts, gids, data):
+        import torch
         gids = gids.to(self.device).contiguous()
         data = data.to(self.device).contiguous()
+        # the received rows were made on torch's stream (an NCCL receive, or a
+        # copy from host memory and a cat); the batch reads them on its own
+        torch.cuda.current_stream(self.device).synchronize()
         self.batch.unpack_cells(cells, np.asarray(counts, np.uint32), gids.data_ptr(), data.data_ptr())
 
 
