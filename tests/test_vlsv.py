@@ -37,5 +37,14 @@ def test_vlasov_file_round_trip(tmp_path):
     np.testing.assert_array_equal(r.read("MESH_BBOX", mesh="proton"), [67, 67, 67, 4, 4, 4])
     crd = r.read("MESH_NODE_CRDS_X", mesh="proton")
     assert len(crd) == 67 * 4 + 1 and crd[0] == mesh.vmin[0]
+    # what the reference's restart reader looks up first (ioread.cpp:170-200, 1162-1194)
+    np.testing.assert_array_equal(r.read("VARIABLE", name="CellID", mesh="SpatialGrid"), np.arange(1, 5))
+    assert r.find("VARIABLE", name="CellID").get("vectorsize") == "1"
+    for name, want, kind, size in (("time", 0.0, "float", "8"), ("timestep", 0, "uint", "4"),
+                                   ("xmax", 6e5, "float", "8"), ("ycells_ini", 2, "uint", "4"),
+                                   ("zcells_ini", 1, "uint", "4")):
+        el = r.find("PARAMETER", name=name)
+        assert (el.get("datatype"), el.get("datasize"), el.get("arraysize")) == (kind, size, "1"), name
+        assert r.read("PARAMETER", name=name)[0] == want, name
     np.testing.assert_allclose(r.read("VARIABLE", name="vg_v"), mom[:, 5:8])
     np.testing.assert_allclose(r.read("VARIABLE", name="vg_pressure"), mom[:, 9:12].mean(1))

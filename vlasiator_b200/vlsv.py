@@ -10,7 +10,10 @@ and whose mandatory attributes are arraysize, vectorsize, datatype
 not part of its tree, so files are checked against that specification and by
 reading them back, not against the library's reader.
 
-Arrays of a Vlasov file (iowrite.cpp:141-320, 690-715; datareducer.cpp):
+Arrays of a Vlasov file (iowrite.cpp:141-320, 485-555, 690-715;
+datareducer.cpp): the CellID variable and the scalar PARAMETER arrays
+(time, dt, timestep, the grid's extent and cell counts) that the
+reference's restart reader looks up (ioread.cpp:170-200, 1162-1194);
 MESH / MESH_BBOX / MESH_NODE_CRDS_{X,Y,Z} of the spatial grid
 ("SpatialGrid"), the same for each population's velocity mesh, and per
 population CELLSWITHBLOCKS, BLOCKSPERCELL, BLOCKIDS and BLOCKVARIABLE (the
@@ -98,14 +101,30 @@ def _node_coords(vmin, cell, n_cells):
 
 def write_vlasov_file(path: str, mesh: VelocityMesh, cells, grid_dims=None, dx=(3e5, 3e5, 3e5),
                       grid_min=(0.0, 0.0, 0.0), moments=None, pop: str = "proton", mass: float | None = None,
-                      charge: float | None = None) -> None:
+                      charge: float | None = None, time: float = 0.0, dt: float = 0.0, timestep: int = 0,
+                      file_index: int = 0) -> None:
     """One population's VDF and moments.  cells: [(gids, data)] per spatial
     cell, x fastest (cell ID = index + 1, as dccrg numbers a uniform grid);
-    moments: the batch's (n_cells, 16) record (vlgpu_batch_moments)."""
+    moments: the batch's (n_cells, 16) record (vlgpu_batch_moments); time,
+    dt, timestep and file_index: the run's scalar parameters."""
     n = len(cells)
     dims = tuple(grid_dims) if grid_dims is not None else (n, 1, 1)
     ids = np.arange(1, n + 1, dtype=np.uint64)
     with VlsvWriter(path) as w:
+        # the cell IDs and the run's scalar parameters (writeCommonGridData,
+        # iowrite.cpp:485-514): Real parameters as float64, uint ones as uint32
+        w.write_array("VARIABLE", {"name": "CellID", "mesh": "SpatialGrid"}, ids)
+        lo = np.asarray(grid_min, np.float64)
+        hi = lo + np.asarray(dx, np.float64) * np.asarray(dims, np.float64)
+        for name, value, dtype in (("time", time, np.float64), ("dt", dt, np.float64),
+                                   ("timestep", timestep, np.uint32), ("fieldSolverSubcycles", 1, np.uint32),
+                                   ("fileIndex", file_index, np.uint32),
+                                   ("xmin", lo[0], np.float64), ("xmax", hi[0], np.float64),
+                                   ("ymin", lo[1], np.float64), ("ymax", hi[1], np.float64),
+                                   ("zmin", lo[2], np.float64), ("zmax", hi[2], np.float64),
+                                   ("xcells_ini", dims[0], np.uint32), ("ycells_ini", dims[1], np.uint32),
+                                   ("zcells_ini", dims[2], np.uint32)):
+            w.write_array("PARAMETER", {"name": name}, np.array([value], dtype))
         sg = {"name": "SpatialGrid", "type": "amr_ucd", "max_refinement_level": "0",
               "xperiodic": "yes", "yperiodic": "yes", "zperiodic": "yes"}
         w.write_array("MESH", sg, ids)
@@ -142,7 +161,8 @@ def write_vlasov_file(path: str, mesh: VelocityMesh, cells, grid_dims=None, dx=(
                           m[:, 12:15])
 
 
-def write_batch(path: str, batch, grid_dims=None, dx=(3e5, 3e5, 3e5), pop: str = "proton") -> None:
-    """Downloads a batch (blocks sorted by ID per cell) and its moments and writes them."""
+def write_batch(path: str, batch, grid_dims=None, dx=(3e5, 3e5, 3e5), pop: str = "proton", **params) -> None:
+    """Downloads a batch (blocks sorted by ID per cell) and its moments and
+    writes them; params: write_vlasov_file's time, dt, timestep, file_index."""
     write_vlasov_file(path, batch.mesh, batch.cells(), grid_dims=grid_dims, dx=dx,
-                      moments=batch.moments(second=True), pop=pop)
+                      moments=batch.moments(second=True), pop=pop, **params)
