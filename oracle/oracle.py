@@ -211,6 +211,19 @@ class Restatement:
                                  np.concatenate([d for _, d in state]), dim, dt, dx[dim], min_value)
             state = [(g, out[offs[c]:offs[c + 1]]) for c, (g, _) in enumerate(state)]
         mom_r = np.stack([self.moments(mesh, g, d, mass, charge, second=True) for g, d in state])
+        adjusted, loss, mom_v, isects = self.accelerate_grid(mesh, grid, state, B, dt, map_order, mass, charge,
+                                                             min_value, add_width, hall_min_rhoq, mu0)
+        return adjusted, loss, mom_r, mom_v, isects
+
+    def accelerate_grid(self, mesh: VelocityMesh, grid, cells, B, dt, map_order, mass, charge, min_value=1e-15,
+                        add_width=1, hall_min_rhoq=1.60217653e-19, mu0=1.25663706e-6):
+        """calculateAcceleration of a uniform periodic grid for one subcycle
+        (vlasovmover.cpp:410-475: moments_V, transform, intersections, three
+        map_1d per cell), its final adjustVelocityBlocks with the spatial
+        neighbours and calculateMoments_V (vlasovmover.cpp:564-569).
+        cells: [(gids, data)] x fastest.  Returns (cells sorted by GID, loss
+        per cell, moments_V, intersections)."""
+        state = [(np.asarray(g, np.uint32), np.asarray(d, self.realf).reshape(-1, WID3)) for g, d in cells]
         swept, isects = [], []
         for c, (g, d) in enumerate(state):
             m0 = self.moments(mesh, g, d, mass, charge, second=False)
@@ -223,7 +236,7 @@ class Restatement:
             isects.append(isect)
         adjusted, loss = self.adjust_grid(mesh, grid, swept, min_value, add_width)
         mom_v = np.stack([self.moments(mesh, g, d, mass, charge, second=True) for g, d in adjusted])
-        return adjusted, loss, mom_r, mom_v, np.stack(isects)
+        return adjusted, loss, mom_v, np.stack(isects)
 
     def acceleration_transform(self, B, curl, rhoq, V, egradpe, q, m, dt, hall_min_rhoq, ohm_gradpe, mu0):
         L = np.zeros(9)

@@ -1,9 +1,10 @@
 """The y-slab ghost exchange of a sharded grid (vlasiator_b200/halo.py) on the
 host, with two (and three) gloo ranks, one process each: the slab
 bookkeeping, the exchange itself (ghost rows filled with the neighbouring
-slabs' owned rows across the periodic wrap), and the translation z, x,
+slabs' owned rows across the periodic wrap), the translation z, x,
 exchange, y of every slab with the oracle against the same translation of
-the whole grid (bit-identical owned cells).  The slabs' cells live in numpy
+the whole grid (bit-identical owned cells), and whole Vlasov steps of the
+slabs with three ghost rows and two exchanges, or four and one.  The slabs' cells live in numpy
 here; on a GPU the same exchange runs over batches
 (tests/test_gpu_halo.py)."""
 import os
@@ -98,6 +99,77 @@ def _rank_main(rank, world, port, dims, out):
         dist.destroy_process_group()
 
 
+def _rank_step(rank, world, port, dims, ghost, out):
+    """A whole Vlasov step of rank's slab with the oracle: translation z, x,
+    exchange, y, (exchange,) acceleration with the adjustment over the 26
+    neighbours; against the same step of the whole grid."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    import torch.distributed as dist
+    from grid_cases import r_dt_restated, varied_grid
+    from oracle.oracle import Restatement
+    from vlasiator_b200.halo import GHOST_ONE_EXCHANGE, exchange_ghosts
+    from vlasiator_b200.mesh import CHARGE, MASS_PROTON, VelocityMesh
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        mesh = VelocityMesh()
+        cells = varied_grid(mesh, dims, seed=3)
+        whole = [(c.gids, c.data) for c in cells]
+        B = np.stack([c.B for c in cells])
+        orc = Restatement("sp")
+        dt = 0.8 * float(r_dt_restated(mesh, cells, (DX, DX, DX)).min())
+        ref, ref_loss, _, ref_mom, _ = orc.vlasov_step(mesh, dims, whole, B, dt, 1, (DX, DX, DX), MASS_PROTON, CHARGE)
+        translated = whole
+        for dim in (2, 0, 1):
+            translated = _translate(orc, mesh, dims, translated, dim, dt)
+        slab = Slab(dims, rank, world, ghost)
+        glob = slab.local_cells_global()
+        side = HostSide([whole[g] for g in glob])
+        for dim in (2, 0):
+            side.cells = _translate(orc, mesh, slab.local_dims, side.cells, dim, dt)
+        exchange_ghosts(side, slab)
+        side.cells = _translate(orc, mesh, slab.local_dims, side.cells, 1, dt)
+        # the ghost rows next to the owned ones, which the owned cells' adjustment reads
+        inner = np.concatenate([slab.rows([ghost - 1]), slab.rows([ghost + slab.n_own])])
+        inner_current = all(np.array_equal(side.cells[c][1], translated[glob[c]][1]) for c in inner)
+        exchanges = 1
+        if ghost < GHOST_ONE_EXCHANGE:
+            exchange_ghosts(side, slab)
+            exchanges += 1
+        got, loss, mom, _ = orc.accelerate_grid(mesh, slab.local_dims, side.cells, B[glob], dt, 1, MASS_PROTON,
+                                                CHARGE)
+        own = [int(c) for c in slab.owned]
+        cells_equal = all(np.array_equal(got[c][0], ref[glob[c]][0]) and np.array_equal(got[c][1], ref[glob[c]][1])
+                          for c in own)
+        mom_equal = all(np.array_equal(mom[c], ref_mom[glob[c]]) and loss[c] == ref_loss[glob[c]] for c in own)
+        out[rank] = (inner_current, cells_equal, mom_equal, exchanges, len(own))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,ghost", [(2, 3), (2, 4), (3, 4)])
+def test_sharded_vlasov_step_matches_the_whole_grid(world, ghost):
+    """Three ghost rows need the second exchange; with four the rows next to
+    the owned ones come out of the y translation current, and one exchange
+    per step gives the same owned cells, moments and RHOLOSSADJUST."""
+    from vlasiator_b200.halo import GHOST_ONE_EXCHANGE
+    dims = (4, 12, 2)
+    port = _free_port()
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that holds CUDA
+        out = m.dict()
+        mp.spawn(_rank_step, args=(world, port, dims, ghost, out), nprocs=world, join=True)
+        res = dict(out)
+    assert sorted(res) == list(range(world))
+    for r, (inner_current, cells_equal, mom_equal, exchanges, _) in res.items():
+        assert exchanges == (1 if ghost >= GHOST_ONE_EXCHANGE else 2)
+        if ghost >= GHOST_ONE_EXCHANGE:
+            assert inner_current, f"rank {r}: the ghost rows next to the owned ones are not current"
+        assert cells_equal, f"rank {r}: owned cells differ from the whole grid's step"
+        assert mom_equal, f"rank {r}: owned moments or RHOLOSSADJUST differ"
+    assert sum(v[4] for v in res.values()) == np.prod(dims)
+
+
 def test_slab_bookkeeping():
     dims = (3, 10, 2)
     slabs = [Slab(dims, r, 3) for r in range(3)]
@@ -112,6 +184,8 @@ def test_slab_bookkeeping():
         assert np.array_equal(s.global_of_local(s.send_down), down.global_of_local(down.recv_up))
     with pytest.raises(ValueError):
         Slab((3, 4, 2), 0, 2)  # two rows per slab cannot supply three ghost rows
+    with pytest.raises(ValueError):
+        Slab((3, 10, 2), 0, 2, ghost=2)  # fewer ghost rows than the translation's stencil reads
 
 
 @pytest.mark.parametrize("world", [2, 3])
