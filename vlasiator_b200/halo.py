@@ -119,13 +119,18 @@ class BatchSide:
         self.batch.unpack_cells(cells, np.asarray(counts, np.uint32), gids.data_ptr(), data.data_ptr())
 
 
-def _p2p(ops_spec, group):
-    """Runs (op, tensor, peer, tag) point-to-point operations as one batch."""
+def _p2p(ops_spec, group, device):
+    """Runs (op, tensor, peer, tag) point-to-point operations as one batch,
+    with `device` current (NCCL launches its transfers on the current GPU)."""
+    import contextlib
+
+    import torch
     import torch.distributed as dist
     ops = [dist.P2POp(dist.isend if kind == "send" else dist.irecv, t, peer, group, tag)
            for kind, t, peer, tag in ops_spec]
-    for req in dist.batch_isend_irecv(ops):
-        req.wait()
+    with torch.cuda.device(device) if device.type == "cuda" else contextlib.nullcontext():
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
 
 
 def exchange_ghosts(side, slab: Slab, group=None) -> None:
@@ -149,7 +154,7 @@ def exchange_ghosts(side, slab: Slab, group=None) -> None:
         r_cd = torch.empty(len(slab.recv_down), dtype=torch.int32, device=comm)
         r_cu = torch.empty(len(slab.recv_up), dtype=torch.int32, device=comm)
         _p2p([("send", t_cu, up, _TAG_UP), ("send", t_cd, down, _TAG_DOWN),
-              ("recv", r_cd, down, _TAG_UP), ("recv", r_cu, up, _TAG_DOWN)], group)
+              ("recv", r_cd, down, _TAG_UP), ("recv", r_cu, up, _TAG_DOWN)], group, comm)
         n_d, n_u = int(r_cd.sum()), int(r_cu.sum())
         # the block IDs and values
         rg_d = torch.empty(max(n_d, 1), dtype=torch.int32, device=comm)
@@ -167,7 +172,7 @@ def exchange_ghosts(side, slab: Slab, group=None) -> None:
         if n_u:
             ops += [("recv", rg_u, up, _TAG_DOWN), ("recv", rv_u, up, _TAG_DOWN)]
         if ops:
-            _p2p(ops, group)
+            _p2p(ops, group, comm)
         rd = (r_cd.cpu().numpy(), rg_d[:n_d], rv_d[:n_d])
         ru = (r_cu.cpu().numpy(), rg_u[:n_u], rv_u[:n_u])
     cells = np.concatenate([slab.recv_down, slab.recv_up])
