@@ -440,7 +440,8 @@ def run_ours(args):
         "gpu_launches": launches,
         "cuda_graph": bool(args.graph),
         "arithmetic": "exact (bit-identical to the reference's map_1d)" if args.exact else
-                      "fused (reference PPM, FMA target distribution; 1e-5 of peak per step)",
+                      "fused (the remap walk: PPM face values once per face, target edges with the "
+                      "reference's rounding; 1e-5 of peak per sweep)",
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                        "what": "device time of one batched acceleration step of all cells"},
         "plain_per_cell": plain,
