@@ -62,6 +62,15 @@ sed -n '1,443p' "$REF/vlasovsolver/cpu_trans_map_amr.cpp" > "$SRC/vlasovsolver/c
   printf '#include <algorithm>\n#include <limits>\n#include <vector>\nusing namespace std;\n'
   cat "$REF/vlasovsolver/arch_dt.cpp"
 } > "$SRC/vlasovsolver/arch_dt_part.cpp"
+# the initial condition's phase-space densities, MaxwellianPhaseSpaceDensity
+# and TriMaxwellianPhaseSpaceDensity (projects/project.h lines 34-73, inline
+# functions), without the Project class and the field-solver headers around them
+mkdir -p "$SRC/projects"
+{
+  printf '#include <cmath>\n#include "common.h"\nnamespace projects {\n'
+  sed -n '34,73p' "$REF/projects/project.h"
+  printf '}  // namespace projects\n'
+} > "$SRC/projects/project_density_part.h"
 cp "$HERE/ref_shim/grid.h" "$SRC/grid.h"
 cp "$HERE/ref_shim/object_wrapper.h" "$SRC/object_wrapper.h"
 cp "$HERE/ref_shim/spatial_cells/spatial_cell_wrapper.hpp" "$SRC/spatial_cells/spatial_cell_wrapper.hpp"

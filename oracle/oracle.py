@@ -312,6 +312,8 @@ class ReferenceBuild:
         L.ref_map_order.argtypes = [ctypes.c_uint32]
         L.ref_cells_content.restype = ctypes.c_uint64
         L.ref_cells_content.argtypes = [_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint8), ctypes.c_uint64]
+        L.ref_fill_blocks.argtypes = [ctypes.c_uint64, _u32p, _dp, ctypes.c_double, _dp, ctypes.c_double,
+                                      ctypes.c_double, ctypes.POINTER(ct)]
 
     def init(self, mesh: VelocityMesh, wall_margin: int = 1):
         vmin = np.array(mesh.vmin, np.float64)
@@ -331,6 +333,19 @@ class ReferenceBuild:
 
     def destroy(self, h):
         self.lib.ref_cells_destroy(h)
+
+    def fill_blocks(self, gids, V, T, rho, mass, T_aniso=None):
+        """The projects' initial fill of the given blocks (the Maxwellian, or
+        with T_aniso = (Tx, Ty, Tz) the axis-aligned tri-Maxwellian, of
+        projects/project.h:45-73 at the cell centres); (n_blocks, 64)."""
+        g = np.ascontiguousarray(gids, np.uint32)
+        v = np.ascontiguousarray(V, np.float64)
+        ta = None if T_aniso is None else np.ascontiguousarray(T_aniso, np.float64)
+        out = np.zeros((len(g), WID3), self.realf)
+        self.lib.ref_fill_blocks(len(g), _ptr(g, ctypes.c_uint32), _ptr(v, ctypes.c_double), float(T),
+                                 None if ta is None else _ptr(ta, ctypes.c_double), float(rho), float(mass),
+                                 _ptr(out, self._ct))
+        return out
 
     def extract(self, h, c, sort=True):
         n = self.lib.ref_cells_block_count(h, c)

@@ -21,6 +21,7 @@
 #include "vlasovsolver/arch_moments.h"
 #include "vlasovsolver/cpu_trans_map_amr.hpp"
 #include "vlasovsolver/cpu_trans_pencils.hpp"
+#include "projects/project_density_part.h"
 
 namespace spatial_cell {
 // the reference's grid-level block adjustment (spatial_cells/block_adjust_cpu.cpp:33-117)
@@ -85,6 +86,35 @@ int ref_init(const double vmin[3], const double vmax[3], const uint32_t grid_len
    }
    Parameters::bailout_velocity_space_wall_margin = wall_margin;
    return 0;
+}
+
+// The initial condition of a list of blocks as the projects' fillPhaseSpace
+// evaluates it (e.g. projects/Distributions/Distributions.cpp:161-178): the
+// block's corner and cell size from VelocityMesh::getBlockInfo, and at each
+// cell centre relative to the bulk velocity V the Maxwellian of temperature T
+// or, with T_aniso (Tx, Ty, Tz) given, the tri-Maxwellian
+// (projects/project.h:45-73).  Values in the cell order k*WID2 + j*WID + i.
+void ref_fill_blocks(uint64_t n_blocks, const uint32_t* gids, const double V[3], double T, const double* T_aniso,
+                     double rho, double mass, Realf* out) {
+   SpatialCell cell(1);
+   cell.get_velocity_mesh(0)->initialize(0);
+   const vmesh::VelocityMesh* vm = cell.get_velocity_mesh(0);
+#pragma omp parallel for schedule(static)
+   for (uint64_t b = 0; b < n_blocks; ++b) {
+      Real c[6];
+      vm->getBlockInfo(gids[b], c);
+      for (uint k = 0; k < WID; ++k)
+         for (uint j = 0; j < WID; ++j)
+            for (uint i = 0; i < WID; ++i) {
+               const Real vx = c[0] + (i + 0.5) * c[3] - V[0];
+               const Real vy = c[1] + (j + 0.5) * c[4] - V[1];
+               const Real vz = c[2] + (k + 0.5) * c[5] - V[2];
+               out[b * WID3 + k * WID2 + j * WID + i] =
+                   T_aniso ? projects::TriMaxwellianPhaseSpaceDensity(vx, vy, vz, T_aniso[0], T_aniso[1], T_aniso[2],
+                                                                      rho, mass)
+                           : projects::MaxwellianPhaseSpaceDensity(vx, vy, vz, T, rho, mass);
+            }
+   }
 }
 
 int ref_bailouts() { return g_bailouts; }
