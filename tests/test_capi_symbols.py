@@ -64,3 +64,20 @@ int main(void) { return vlgpu_version() == 0; }
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
                         str(src), "-L", lib_dir, "-lvlgpu", "-o", str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_entry_points_reject_null_arguments():
+    """Every status-returning entry point, given null pointers and zero sizes,
+    returns VLGPU_EINVAL before it touches the device (so this runs without a
+    GPU): the argument checks come first everywhere."""
+    import ctypes
+    lib = vlgpu.load()
+    checked = 0
+    for name, (res, args) in sorted(vlgpu.SIGNATURES.items()):
+        if res is not ctypes.c_int:
+            continue
+        zeros = [0.0 if a in (ctypes.c_double, ctypes.c_float) else
+                 None if (hasattr(a, "contents") or a in (ctypes.c_void_p, ctypes.c_char_p)) else 0 for a in args]
+        assert getattr(lib, name)(*zeros) == 1, name  # VLGPU_EINVAL
+        checked += 1
+    assert checked >= 45
